@@ -1,0 +1,251 @@
+// aux_kernels.cu -- initialisation, obstacle rasterisation, macroscopic fields, FP64
+// statistics and FP64 <-> storage conversion.  Compiled with --fmad=false so that the
+// obstacle tests and the initial populations round exactly like the reference's.
+#include <cuda_runtime.h>
+
+#include "aux_kernels.cuh"
+#include "lbm_step.cuh"
+
+namespace hlbm {
+
+// ------------------------------------------------------------------ set_distribution
+// init_distributions (set_distribution.hpp:39-42): f_i = value * w_i on a box of nodes.
+template <typename S, typename R>
+__global__ void k_set_distribution(S* f, int64_t stride, int nx, int ny, int lo0, int lo1, int lo2, int hx,
+                                   int hy, int hz, double value, const StepPlan p) {
+  const int x = lo0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = lo1 + blockIdx.y;
+  const int z = lo2 + blockIdx.z;
+  if (x > hx || y > hy || z > hz) return;
+  const int64_t idx = ((int64_t)z * ny + y) * nx + x;
+  Unroll<0, Q>::run([&]<int I>() {
+    const double v = value * (1.0 / D3Q19::wden[I]);
+    f[I * stride + idx] = Codec<S, R>::template enc<I>(R(v), p);
+  });
+}
+
+// ------------------------------------------------------------------ obstacles
+// SetObstacleFunc (update_obstacles.cu:32-45): the node at real (x, y, z) sits at
+// ((x + 2) - 2) * dx (compute_position<Global>, grid.hpp:355-361: the origin is not added).
+__global__ void k_rasterize(int8_t* flags, int nx, int ny, int lo0, int lo1, int lo2, int hx, int hy, int hz,
+                            double dx, ObstacleDesc o) {
+  const int x = lo0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = lo1 + blockIdx.y;
+  const int z = lo2 + blockIdx.z;
+  if (x > hx || y > hy || z > hz) return;
+  const double px = ((double)(x + 2) + (double)(-2)) * dx;
+  const double py = ((double)(y + 2) + (double)(-2)) * dx;
+  const double pz = ((double)(z + 2) + (double)(-2)) * dx;
+  bool solid = false;
+  if (o.type == OBS_BALL) {  // Ball::solid (obstacle.hpp:59-62)
+    const double rx = px - o.a[0], ry = py - o.a[1], rz = pz - o.a[2];
+    solid = rx * rx + ry * ry + rz * rz <= o.a[4];
+  } else if (o.type == OBS_WALL) {  // intersect (obstacle.hpp:13-17): strict interior
+    solid = o.a[0] < px && px < o.a[3] && o.a[1] < py && py < o.a[4] && o.a[2] < pz && pz < o.a[5];
+  } else if (o.type == OBS_QUADRIC) {  // p^T Q p <= 0 with p = (x, y, z, 1)
+    const double pv[4] = {px, py, pz, 1.0};
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      double row = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) row = row + o.a[i * 4 + j] * pv[j];
+      acc = acc + pv[i] * row;
+    }
+    solid = acc <= 0.0;
+  }
+  if (solid) flags[((int64_t)z * ny + y) * nx + x] = FLAG_WALL;
+}
+
+// ------------------------------------------------------------------ macro + statistics
+// macro_variables (macro_variables.hpp:48-79) on a state S_k, in FP64, plus the per-block
+// partials of simulation_state (simulation_state.hpp:47-54): sum rho, min |u|, max |u|.
+// Walls keep rho = 0 and u = 0 (macro_variables never writes their m0).
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_macro_stats(const S* __restrict__ f, const int8_t* __restrict__ flags,
+                                                     int64_t ncell, double* __restrict__ rho_out,
+                                                     double* __restrict__ u_out, double* __restrict__ partials,
+                                                     const StepPlan p) {
+  double s = 0.0, vmin = 1.79769313486231570815e+308, vmax = -1.79769313486231570815e+308;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < ncell;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    double rho = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+    if (flags[idx] >= FLAG_FLUID) {
+      double v[Q];
+      Unroll<0, Q>::run([&]<int I>() { v[I] = double(Codec<S, R>::template dec<I>(f[I * p.stride + idx], p)); });
+      macro<double, true>(v, rho, ux, uy, uz);
+    }
+    if (rho_out) rho_out[idx] = rho;
+    if (u_out) {
+      u_out[idx] = ux;
+      u_out[ncell + idx] = uy;
+      u_out[2 * ncell + idx] = uz;
+    }
+    s += rho;
+    const double n = sqrt(ux * ux + uy * uy + uz * uz);
+    vmin = n < vmin ? n : vmin;
+    vmax = n > vmax ? n : vmax;
+  }
+  // warp then block reduction (fixed order: deterministic for a fixed launch shape)
+  for (int off = 16; off > 0; off >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, off);
+    const double a = __shfl_down_sync(0xffffffffu, vmin, off);
+    const double b = __shfl_down_sync(0xffffffffu, vmax, off);
+    vmin = a < vmin ? a : vmin;
+    vmax = b > vmax ? b : vmax;
+  }
+  __shared__ double sh[3][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    sh[0][warp] = s;
+    sh[1][warp] = vmin;
+    sh[2][warp] = vmax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    double a = sh[0][0], b = sh[1][0], c = sh[2][0];
+    for (int w = 1; w < nw; w++) {
+      a += sh[0][w];
+      b = sh[1][w] < b ? sh[1][w] : b;
+      c = sh[2][w] > c ? sh[2][w] : c;
+    }
+    partials[3 * blockIdx.x + 0] = a;
+    partials[3 * blockIdx.x + 1] = b;
+    partials[3 * blockIdx.x + 2] = c;
+  }
+}
+
+// second pass: one block folds the per-block partials in block order
+__global__ void k_reduce_partials(const double* __restrict__ partials, int nparts, double* __restrict__ out) {
+  __shared__ double sh[3][256];
+  double s = 0.0, vmin = 1.79769313486231570815e+308, vmax = -1.79769313486231570815e+308;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    s += partials[3 * i];
+    vmin = partials[3 * i + 1] < vmin ? partials[3 * i + 1] : vmin;
+    vmax = partials[3 * i + 2] > vmax ? partials[3 * i + 2] : vmax;
+  }
+  sh[0][threadIdx.x] = s;
+  sh[1][threadIdx.x] = vmin;
+  sh[2][threadIdx.x] = vmax;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + h];
+      sh[1][threadIdx.x] = sh[1][threadIdx.x + h] < sh[1][threadIdx.x] ? sh[1][threadIdx.x + h] : sh[1][threadIdx.x];
+      sh[2][threadIdx.x] = sh[2][threadIdx.x + h] > sh[2][threadIdx.x] ? sh[2][threadIdx.x + h] : sh[2][threadIdx.x];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sh[0][0];
+    out[1] = sh[1][0];
+    out[2] = sh[2][0];
+  }
+}
+
+// ------------------------------------------------------------------ FP64 <-> storage
+template <typename S, typename R, int I>
+__device__ __forceinline__ void dec_plane(const S* f, double* out, int64_t n, const StepPlan& p) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = double(Codec<S, R>::template dec<I>(f[I * p.stride + i], p));
+}
+template <typename S, typename R>
+__global__ void k_decode(const S* __restrict__ f, double* __restrict__ out, int dir, int64_t n, const StepPlan p) {
+  Unroll<0, Q>::run([&]<int I>() {
+    if (I == dir) dec_plane<S, R, I>(f, out, n, p);
+  });
+}
+template <typename S, typename R>
+__global__ void k_encode(S* __restrict__ f, const double* __restrict__ in, int dir, int64_t n, const StepPlan p) {
+  Unroll<0, Q>::run([&]<int I>() {
+    if (I != dir) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      f[I * p.stride + i] = Codec<S, R>::template enc<I>(R(in[i]), p);
+  });
+}
+
+// ------------------------------------------------------------------ host launchers
+template <typename S, typename R>
+static cudaError_t set_dist_t(void* f, const StepPlan& p, const int lo[3], const int hi[3], double value,
+                              cudaStream_t s) {
+  const int w = hi[0] - lo[0] + 1;
+  dim3 block(w >= 128 ? 128 : ((w + 31) / 32) * 32), grid((w + block.x - 1) / block.x, hi[1] - lo[1] + 1,
+                                                             hi[2] - lo[2] + 1);
+  k_set_distribution<S, R><<<grid, block, 0, s>>>(static_cast<S*>(f), p.stride, p.nx, p.ny, lo[0], lo[1], lo[2],
+                                                  hi[0], hi[1], hi[2], value, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_distribution(int prec, void* f, const StepPlan& p, const int lo[3], const int hi[3],
+                                    double value, cudaStream_t s) {
+  switch (prec) {
+    case 0:
+    case 1: return set_dist_t<double, double>(f, p, lo, hi, value, s);
+    case 2: return set_dist_t<float, float>(f, p, lo, hi, value, s);
+    case 3: return set_dist_t<__half, float>(f, p, lo, hi, value, s);
+    default: return set_dist_t<__nv_bfloat16, float>(f, p, lo, hi, value, s);
+  }
+}
+
+cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], const int hi[3], double dx,
+                             const ObstacleDesc& o, cudaStream_t s) {
+  const int w = hi[0] - lo[0] + 1;
+  dim3 block(w >= 128 ? 128 : ((w + 31) / 32) * 32), grid((w + block.x - 1) / block.x, hi[1] - lo[1] + 1,
+                                                             hi[2] - lo[2] + 1);
+  k_rasterize<<<grid, block, 0, s>>>(flags, p.nx, p.ny, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], dx, o);
+  return cudaGetLastError();
+}
+
+int stats_blocks(int64_t ncell) {
+  int64_t b = (ncell + 255) / 256;
+  return int(b < 148 * 8 ? b : 148 * 8);
+}
+
+template <typename S, typename R>
+static cudaError_t macro_stats_t(const void* f, const int8_t* flags, const StepPlan& p, double* rho, double* u,
+                                 double* partials, double* out3, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  k_macro_stats<S, R><<<nb, 256, 0, s>>>(static_cast<const S*>(f), flags, p.ncell, rho, u, partials, p);
+  k_reduce_partials<<<1, 256, 0, s>>>(partials, nb, out3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_macro_stats(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* rho,
+                               double* u, double* partials, double* out3, cudaStream_t s) {
+  switch (prec) {
+    case 0:
+    case 1: return macro_stats_t<double, double>(f, flags, p, rho, u, partials, out3, s);
+    case 2: return macro_stats_t<float, float>(f, flags, p, rho, u, partials, out3, s);
+    case 3: return macro_stats_t<__half, float>(f, flags, p, rho, u, partials, out3, s);
+    default: return macro_stats_t<__nv_bfloat16, float>(f, flags, p, rho, u, partials, out3, s);
+  }
+}
+
+cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  switch (prec) {
+    case 2: k_decode<float, float><<<nb, 256, 0, s>>>(static_cast<const float*>(f), out, dir, p.ncell, p); break;
+    case 3: k_decode<__half, float><<<nb, 256, 0, s>>>(static_cast<const __half*>(f), out, dir, p.ncell, p); break;
+    case 4:
+      k_decode<__nv_bfloat16, float><<<nb, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(f), out, dir, p.ncell, p);
+      break;
+    default: k_decode<double, double><<<nb, 256, 0, s>>>(static_cast<const double*>(f), out, dir, p.ncell, p); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_encode(int prec, void* f, const double* in, int dir, const StepPlan& p, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  switch (prec) {
+    case 2: k_encode<float, float><<<nb, 256, 0, s>>>(static_cast<float*>(f), in, dir, p.ncell, p); break;
+    case 3: k_encode<__half, float><<<nb, 256, 0, s>>>(static_cast<__half*>(f), in, dir, p.ncell, p); break;
+    case 4:
+      k_encode<__nv_bfloat16, float><<<nb, 256, 0, s>>>(static_cast<__nv_bfloat16*>(f), in, dir, p.ncell, p);
+      break;
+    default: k_encode<double, double><<<nb, 256, 0, s>>>(static_cast<double*>(f), in, dir, p.ncell, p); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace hlbm

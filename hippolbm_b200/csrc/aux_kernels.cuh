@@ -1,0 +1,27 @@
+// aux_kernels.cuh -- launchers for the non-step kernels (see aux_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "d3q19.cuh"
+
+namespace hlbm {
+
+enum ObstacleType : int32_t { OBS_NONE = -1, OBS_BALL = 0, OBS_WALL = 1, OBS_QUADRIC = 2 };
+
+// Ball: a = {cx, cy, cz, r, r*r}; Wall: a = {min xyz, max xyz}; Quadric: a = Q row-major.
+struct ObstacleDesc {
+  int32_t type;
+  double a[16];
+};
+
+cudaError_t launch_set_distribution(int prec, void* f, const StepPlan& p, const int lo[3], const int hi[3],
+                                    double value, cudaStream_t s);
+cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], const int hi[3], double dx,
+                             const ObstacleDesc& o, cudaStream_t s);
+int stats_blocks(int64_t ncell);
+cudaError_t launch_macro_stats(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* rho,
+                               double* u, double* partials, double* out3, cudaStream_t s);
+cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s);
+cudaError_t launch_encode(int prec, void* f, const double* in, int dir, const StepPlan& p, cudaStream_t s);
+
+}  // namespace hlbm

@@ -1,0 +1,700 @@
+// capi.cu -- host runtime behind include/hippolbm.h.
+//
+// A context owns one lattice on one device: two SoA population buffers (pull scheme), one
+// flag byte per node, a step plan compiled from the recorded hook operators, and a stream.
+// State phases:
+//   RAW     f[cur] holds S_k, the reference's state after k steps (post-stream + BCs);
+//   POSTCOL f[cur] holds C_{k-1}, the post-collision state inside step k (what the fused
+//           kernel carries from launch to launch);
+//   MATER   as POSTCOL, and f[1-cur] also holds S_k, produced by the finish kernel for a
+//           read-out (the next step overwrites it).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "hippolbm.h"
+#include "launch.cuh"
+
+using namespace hlbm;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define HLBM_CK(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(HLBM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+enum HookKind { H_PRE_BB, H_CAVITY, H_WALL_BB, H_POST_BB, H_NEUMANN, H_LID, H_SETDIST };
+
+struct HookOp {
+  int hook;
+  int kind;
+  int face;  // cavity side (0, 1) or plane face (0..5)
+  double u[3];
+  double value;
+  double bounds[6];
+};
+
+enum Phase { RAW = 0, POSTCOL = 1, MATER = 2 };
+
+size_t elem_size(int prec) {
+  switch (prec) {
+    case HLBM_F64:
+    case HLBM_F64_STRICT: return 8;
+    case HLBM_F32: return 4;
+    default: return 2;
+  }
+}
+
+constexpr double W_OF(int i) { return 1.0 / D3Q19::wden[i]; }
+}  // namespace
+
+struct hlbm_ctx {
+  int n[3];
+  int periodic[3];
+  double bmin[3], bmax[3], dx;
+  int precision;
+  int device;
+  // LBMParameters (lbm_parameters.hpp:41-57)
+  double Fext[3], celerity, dtLB, nuth, nu, tau, avg_rho;
+  int collision = 0;
+  double mrt[8];
+  double rho0 = 1.0, scale = 1.0;
+  std::vector<HookOp> hooks;
+  std::vector<ObstacleDesc> obstacles;
+  void* f[2] = {nullptr, nullptr};
+  int cur = 0;
+  int8_t* flags = nullptr;
+  double* partials = nullptr;
+  double* stats_dev = nullptr;
+  double* plane_tmp = nullptr;
+  cudaStream_t stream = nullptr;
+  int phase = RAW;
+  int64_t steps = 0;
+  int64_t launches = 0;
+  int64_t ncell = 0, stride = 0;
+  StepPlan plan;
+  bool plan_dirty = true;
+};
+
+namespace {
+
+void mrt_reference(double r[8]) {  // mrt.hpp:43-47
+  r[0] = 1.19;
+  r[1] = 1.4;
+  r[2] = 1.2;
+  r[3] = 1.4;
+  r[4] = 1.98;
+  r[5] = 0;
+  r[6] = -475. / 63.;
+  r[7] = 0;
+}
+
+void base_plan(hlbm_ctx* c, StepPlan& p) {
+  std::memset(&p, 0, sizeof(p));
+  p.nx = c->n[0];
+  p.ny = c->n[1];
+  p.nz = c->n[2];
+  for (int d = 0; d < 3; d++) p.periodic[d] = c->periodic[d];
+  p.ncell = c->ncell;
+  p.stride = c->stride;
+  p.rho0 = c->rho0;
+  p.scale = c->scale;
+  p.inv_scale = 1.0 / c->scale;
+}
+
+// the box {int(min / dx), int(max / dx)} of set_distribution / update_obstacles in real
+// coordinates, clipped to the lattice (restrict_box_to_grid, grid.hpp:406-428)
+bool clip_box(const hlbm_ctx* c, const double mn[3], const double mx[3], int lo[3], int hi[3]) {
+  for (int d = 0; d < 3; d++) {
+    lo[d] = int(mn[d] / c->dx);
+    hi[d] = int(mx[d] / c->dx);
+    if (hi[d] < 0 || lo[d] > c->n[d] - 1) return false;
+  }
+  for (int d = 0; d < 3; d++) {
+    lo[d] = lo[d] < 0 ? 0 : lo[d];
+    hi[d] = hi[d] > c->n[d] - 1 ? c->n[d] - 1 : hi[d];
+  }
+  return true;
+}
+
+int build_plan(hlbm_ctx* c) {
+  if (!c->plan_dirty) return HLBM_OK;
+  StepPlan& p = c->plan;
+  base_plan(c, p);
+  p.collision = c->collision;
+  p.tau = c->tau;
+  p.inv_tau = 1.0 / c->tau;
+  for (int d = 0; d < 3; d++) p.F[d] = c->Fext[d];
+  p.has_force = (c->Fext[0] != 0.0 || c->Fext[1] != 0.0 || c->Fext[2] != 0.0) ? 1 : 0;
+  for (int k = 0; k < 8; k++) p.mrt[k] = c->mrt[k];
+  bool pre_seen = false;
+  for (const HookOp& h : c->hooks) {
+    if (h.hook == HLBM_HOOK_PRE_STREAM) {
+      if (h.kind == H_PRE_BB) {
+        pre_seen = true;
+      } else if (h.kind == H_WALL_BB) {
+        p.walls = 1;
+      } else if (h.kind == H_CAVITY) {
+        // cavity<DIMZ,S,19>::compute_coeff (cavity.hpp:55-72): L = nodes along z
+        const int face = h.face ? 5 : 4;
+        if (!pre_seen || c->periodic[2]) continue;  // edits a buffer that pre_bounce_back rewrites / none
+        if (p.ncav[face] >= MAX_CAVITY) return fail(HLBM_EPLAN, "too many cavity operators on one face");
+        static const int ids[2][5] = {{5, 14, 11, 18, 15}, {6, 13, 12, 17, 16}};
+        const double L = c->n[2];
+        const double uxx = h.u[0] * (1 + 0.5 / (L - 1));
+        const double uyy = h.u[1] * (1 + 0.5 / (L - 1));
+        const double uzz = h.u[2] * (1 + 0.5 / (L - 1));
+        for (int k = 0; k < 5; k++) {
+          const int i = ids[h.face ? 1 : 0][k];
+          p.cav[face][p.ncav[face]][k] =
+              6. * W_OF(i) * (D3Q19::ex[i] * uxx + D3Q19::ey[i] * uyy + D3Q19::ez[i] * uzz);
+        }
+        p.ncav[face]++;
+      }
+    }
+  }
+  for (int stage : {HLBM_HOOK_POST_STREAM, HLBM_HOOK_BOUNDARY_CONDITIONS}) {
+    for (const HookOp& h : c->hooks) {
+      if (h.hook != stage) continue;
+      if (p.nops >= MAX_PLANE_OPS) return fail(HLBM_EPLAN, "too many boundary operators");
+      PlaneOp& op = p.ops[p.nops];
+      if (h.kind == H_POST_BB) {
+        if (!pre_seen)
+          return fail(HLBM_EPLAN,
+                      "post_bounce_back needs pre_bounce_back in pre_stream_bcs (it restores the saved populations)");
+        op.kind = OP_POST_BB;
+        op.face = 0;
+      } else {
+        op.kind = h.kind == H_LID ? OP_LID : OP_ZOUHE;
+        op.face = h.face;
+        for (int d = 0; d < 3; d++) op.u[d] = h.u[d] / c->celerity;  // convert_velocity<LBM_UNITS>
+      }
+      p.nops++;
+    }
+  }
+  for (const HookOp& h : c->hooks) {
+    if (h.hook != HLBM_HOOK_START_ITERATION) continue;
+    int lo[3], hi[3];
+    if (!clip_box(c, h.bounds, h.bounds + 3, lo, hi)) continue;
+    if (p.nsets >= MAX_SETS) return fail(HLBM_EPLAN, "too many start_iteration set_distribution operators");
+    SetBox& b = p.sets[p.nsets++];
+    for (int d = 0; d < 3; d++) {
+      b.lo[d] = lo[d];
+      b.hi[d] = hi[d];
+    }
+    b.value = h.value;
+  }
+  c->plan_dirty = false;
+  return HLBM_OK;
+}
+
+cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fout) {
+  const StepPlan& p = c->plan;
+  const int walls = p.walls;
+  c->launches++;
+  switch (c->precision) {
+    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream);
+    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream);
+    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream);
+    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream);
+    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream);
+  }
+}
+
+// make S_k available; returns the buffer holding it
+int state_buffer(hlbm_ctx* c, void** out) {
+  if (c->phase == RAW) {
+    *out = c->f[c->cur];
+    return HLBM_OK;
+  }
+  if (c->phase == POSTCOL) {
+    int rc = build_plan(c);
+    if (rc) return rc;
+    HLBM_CK(launch_step_kernel(c, MODE_FINISH, c->f[c->cur], c->f[1 - c->cur]));
+    c->phase = MATER;
+  }
+  *out = c->f[1 - c->cur];
+  return HLBM_OK;
+}
+
+// turn the context into RAW (S_k in f[cur]) so that S can be edited in place
+int make_raw(hlbm_ctx* c) {
+  if (c->phase == RAW) return HLBM_OK;
+  void* s;
+  int rc = state_buffer(c, &s);
+  if (rc) return rc;
+  c->cur = 1 - c->cur;
+  c->phase = RAW;
+  return HLBM_OK;
+}
+
+int set_device(hlbm_ctx* c) {
+  HLBM_CK(cudaSetDevice(c->device));
+  return HLBM_OK;
+}
+
+int add_hook(hlbm_ctx* c, HookOp h) {
+  c->hooks.push_back(h);
+  c->plan_dirty = true;
+  return HLBM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* hlbm_last_error(void) { return g_err.c_str(); }
+const char* hlbm_version(void) { return "hippolbm-b200 0.1.0 (sm_100a)"; }
+
+int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],
+                int32_t precision, int32_t device, hlbm_ctx** out) {
+  if (!cell_dims || !bmin || !bmax || !periodic || !out) return fail(HLBM_EINVAL, "hlbm_domain: NULL argument");
+  *out = nullptr;
+  if (precision < HLBM_F64 || precision > HLBM_BF16) return fail(HLBM_EINVAL, "hlbm_domain: unknown precision");
+  int n[3];
+  for (int d = 0; d < 3; d++) {
+    if (cell_dims[d] < 1) return fail(HLBM_EDOMAIN, "[Error, domain], cell_dims must be >= 1");
+    n[d] = cell_dims[d] + 1;  // domain_lbm.cpp:68
+  }
+  double reso[3];
+  for (int d = 0; d < 3; d++) reso[d] = (bmax[d] - bmin[d]) / double(n[d] - 1);
+  if (reso[0] != reso[1] || reso[0] != reso[2]) return fail(HLBM_EDOMAIN, "[Error, domain], Dx is not the same for all dimension");
+  for (int d = 0; d < 3; d++)
+    if (bmin[d] + (n[d] - 1) * reso[0] != bmax[d])
+      return fail(HLBM_EDOMAIN, "[Error, domain], The resolution slot and bounds slot mismatch.");
+  auto* c = new hlbm_ctx();
+  for (int d = 0; d < 3; d++) {
+    c->n[d] = n[d];
+    c->periodic[d] = periodic[d] ? 1 : 0;
+    c->bmin[d] = bmin[d];
+    c->bmax[d] = bmax[d];
+  }
+  c->dx = (bmax[0] - bmin[0]) / double(n[0] - 1);  // load_balancing GridDx, make_domain.hpp:280
+  c->precision = precision;
+  c->device = device;
+  c->ncell = int64_t(n[0]) * n[1] * n[2];
+  c->stride = (c->ncell + 127) / 128 * 128;
+  if (precision == HLBM_F16) c->scale = 1024.0;
+  mrt_reference(c->mrt);
+  auto cleanup = [&](int rc) {
+    hlbm_destroy(c);
+    return rc;
+  };
+  if (int rc = set_device(c)) return cleanup(rc);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(HLBM_ECUDA, "cudaStreamCreate failed"));
+  const size_t fbytes = size_t(Q) * c->stride * elem_size(precision);
+  for (int k = 0; k < 2; k++)
+    if (cudaMalloc(&c->f[k], fbytes) != cudaSuccess) {
+      cudaGetLastError();
+      return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate " + std::to_string(fbytes >> 20) +
+                                           " MiB of populations"));
+    }
+  if (cudaMalloc(&c->flags, size_t(c->ncell)) != cudaSuccess ||
+      cudaMalloc(&c->partials, sizeof(double) * 3 * 148 * 8) != cudaSuccess ||
+      cudaMalloc(&c->stats_dev, sizeof(double) * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate flags"));
+  }
+  // init_obst: every flag FLUIDE_ (-1 = 0xff)
+  if (cudaMemsetAsync(c->flags, 0xff, size_t(c->ncell), c->stream) != cudaSuccess)
+    return cleanup(fail(HLBM_ECUDA, "cudaMemsetAsync failed"));
+  // default lbm_parameters slots (lbm_parameters.cpp:57-64)
+  const double F0[3] = {0, 0, 0};
+  if (int rc = hlbm_lbm_parameters(c, F0, 1.0, 1e-4, 1000.0, 0, 0.0, 0.0)) return cleanup(rc);
+  // default set_distribution: value 1 on every node (config_initialize.msp:22-23)
+  if (int rc = hlbm_set_distribution(c, 1.0, nullptr, 0)) return cleanup(rc);
+  *out = c;
+  return HLBM_OK;
+}
+
+int hlbm_destroy(hlbm_ctx* c) {
+  if (!c) return HLBM_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->f[0]);
+  cudaFree(c->f[1]);
+  cudaFree(c->flags);
+  cudaFree(c->partials);
+  cudaFree(c->stats_dev);
+  cudaFree(c->plane_tmp);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return HLBM_OK;
+}
+
+int hlbm_lbm_parameters(hlbm_ctx* c, const double Fext[3], double celerity, double nuth, double avg_rho,
+                        int32_t has_tau, double tau, double dt) {
+  if (!c || !Fext) return fail(HLBM_EINVAL, "hlbm_lbm_parameters: NULL argument");
+  const double dx = c->dx;
+  c->nuth = nuth;
+  c->avg_rho = avg_rho;
+  if (dt > 0.0) {  // define_by_dt (lbm_parameters.hpp:60-66)
+    c->dtLB = dt;
+    c->tau = 3 * c->nuth * c->dtLB / (dx * dx) + 0.5;
+    c->nu = (c->tau - 0.5) / 3.0;
+    c->celerity = dx / c->dtLB;
+  } else if (has_tau) {  // define_by_tau (lbm_parameters.hpp:68-74)
+    c->tau = tau;
+    c->dtLB = dx * dx * (c->tau - 0.5) / (3.0 * c->nuth);
+    c->nu = c->nuth * c->dtLB / (dx * dx);
+    c->celerity = dx / c->dtLB;
+  } else {  // define_by_c (lbm_parameters.hpp:76-81)
+    c->celerity = celerity;
+    c->dtLB = dx / c->celerity;
+    c->nu = c->nuth * c->dtLB / (dx * dx);
+    c->tau = 3. * c->nu + 0.5;
+  }
+  const double ddx = c->celerity * c->dtLB;  // convert_force<LBM_UNITS> (lbm_parameters.hpp:124-128)
+  for (int d = 0; d < 3; d++) c->Fext[d] = Fext[d] * c->dtLB * c->dtLB / ddx;
+  if (!(c->tau > 0.5) || !std::isfinite(c->tau))
+    return fail(HLBM_EINVAL, "hlbm_lbm_parameters: tau = " + std::to_string(c->tau) + " must be > 0.5");
+  c->plan_dirty = true;
+  return HLBM_OK;
+}
+
+int hlbm_get_parameters(hlbm_ctx* c, double out[9]) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_get_parameters: NULL argument");
+  out[0] = c->Fext[0];
+  out[1] = c->Fext[1];
+  out[2] = c->Fext[2];
+  out[3] = c->celerity;
+  out[4] = c->dtLB;
+  out[5] = c->nuth;
+  out[6] = c->nu;
+  out[7] = c->tau;
+  out[8] = c->avg_rho;
+  return HLBM_OK;
+}
+
+int hlbm_collision(hlbm_ctx* c, int32_t kind, const double* rates8) {
+  if (!c || (kind != 0 && kind != 1)) return fail(HLBM_EINVAL, "hlbm_collision: kind must be 0 (bgk) or 1 (mrt)");
+  c->collision = kind;
+  if (rates8)
+    std::memcpy(c->mrt, rates8, sizeof(c->mrt));
+  else
+    mrt_reference(c->mrt);
+  c->plan_dirty = true;
+  return HLBM_OK;
+}
+
+int hlbm_storage_scale(hlbm_ctx* c, double rho0, double scale) {
+  if (!c || !(scale > 0)) return fail(HLBM_EINVAL, "hlbm_storage_scale: scale must be > 0");
+  int rc = make_raw(c);
+  if (rc) return rc;
+  // re-encode the current state under the new deviation parameters
+  std::vector<double> host;
+  if (c->precision == HLBM_F16 || c->precision == HLBM_BF16) {
+    host.resize(size_t(Q) * c->ncell);
+    if ((rc = hlbm_get_populations(c, host.data()))) return rc;
+  }
+  c->rho0 = rho0;
+  c->scale = scale;
+  c->plan_dirty = true;
+  if (!host.empty()) return hlbm_put_populations(c, host.data());
+  return HLBM_OK;
+}
+
+int hlbm_set_distribution(hlbm_ctx* c, double value, const double* bounds6, int32_t /*do_update*/) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_set_distribution: NULL context");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = make_raw(c)) return rc;
+  int lo[3] = {0, 0, 0}, hi[3] = {c->n[0] - 1, c->n[1] - 1, c->n[2] - 1};
+  if (bounds6 && !clip_box(c, bounds6, bounds6 + 3, lo, hi)) return HLBM_OK;
+  StepPlan p;
+  base_plan(c, p);
+  c->launches++;
+  HLBM_CK(launch_set_distribution(c->precision, c->f[c->cur], p, lo, hi, value, c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_init_obstacles(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_init_obstacles: NULL context");
+  c->obstacles.clear();
+  return HLBM_OK;
+}
+
+static ObstacleDesc& obstacle_slot(hlbm_ctx* c, int id) {
+  if (size_t(id) >= c->obstacles.size()) {  // obstacles.hpp:84-107
+    ObstacleDesc none{};
+    none.type = OBS_NONE;
+    c->obstacles.resize(id + 1, none);
+  }
+  return c->obstacles[id];
+}
+
+int hlbm_register_solid_ball(hlbm_ctx* c, int32_t id, const double center[3], double radius) {
+  if (!c || !center || id < 0) return fail(HLBM_EINVAL, "hlbm_register_solid_ball: bad argument");
+  ObstacleDesc& o = obstacle_slot(c, id);
+  o = ObstacleDesc{};
+  o.type = OBS_BALL;
+  o.a[0] = center[0];
+  o.a[1] = center[1];
+  o.a[2] = center[2];
+  o.a[3] = radius;
+  o.a[4] = radius * radius;  // Ball::r2_
+  return HLBM_OK;
+}
+
+int hlbm_register_solid_wall(hlbm_ctx* c, int32_t id, const double bmin[3], const double bmax[3]) {
+  if (!c || !bmin || !bmax || id < 0) return fail(HLBM_EINVAL, "hlbm_register_solid_wall: bad argument");
+  ObstacleDesc& o = obstacle_slot(c, id);
+  o = ObstacleDesc{};
+  o.type = OBS_WALL;
+  for (int d = 0; d < 3; d++) {
+    o.a[d] = bmin[d];
+    o.a[3 + d] = bmax[d];
+  }
+  return HLBM_OK;
+}
+
+int hlbm_register_quadric(hlbm_ctx* c, int32_t id, const double q[16]) {
+  if (!c || !q || id < 0) return fail(HLBM_EINVAL, "hlbm_register_quadric: bad argument");
+  ObstacleDesc& o = obstacle_slot(c, id);
+  o = ObstacleDesc{};
+  o.type = OBS_QUADRIC;
+  std::memcpy(o.a, q, sizeof(double) * 16);
+  return HLBM_OK;
+}
+
+int hlbm_update_obstacles(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_update_obstacles: NULL context");
+  if (int rc = set_device(c)) return rc;
+  StepPlan p;
+  base_plan(c, p);
+  for (const ObstacleDesc& o : c->obstacles) {  // UpdateObstacles::execute (update_obstacles.cu:106-119)
+    if (o.type == OBS_NONE) continue;
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; d++) {
+      if (o.type == OBS_BALL) {  // Ball::covered (obstacle.hpp:46-49)
+        mn[d] = o.a[d] - o.a[3];
+        mx[d] = o.a[d] + o.a[3];
+      } else if (o.type == OBS_WALL) {
+        mn[d] = o.a[d];
+        mx[d] = o.a[3 + d];
+      } else {  // Quadric::covered (obstacle.hpp:119-124)
+        mn[d] = -1e6;
+        mx[d] = 1e6;
+      }
+    }
+    int lo[3], hi[3];
+    if (!clip_box(c, mn, mx, lo, hi)) continue;
+    c->launches++;
+    HLBM_CK(launch_rasterize(c->flags, p, lo, hi, c->dx, o, c->stream));
+  }
+  return HLBM_OK;
+}
+
+int hlbm_clear_hooks(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_clear_hooks: NULL context");
+  c->hooks.clear();
+  c->plan_dirty = true;
+  return HLBM_OK;
+}
+
+int hlbm_pre_bounce_back(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_pre_bounce_back: NULL context");
+  return add_hook(c, HookOp{HLBM_HOOK_PRE_STREAM, H_PRE_BB, 0, {0, 0, 0}, 0, {0}});
+}
+
+int hlbm_cavity(hlbm_ctx* c, int32_t side, const double U[3]) {
+  if (!c || !U || (side != 0 && side != 1)) return fail(HLBM_EINVAL, "hlbm_cavity: side must be 0 (z_0) or 1 (z_l)");
+  return add_hook(c, HookOp{HLBM_HOOK_PRE_STREAM, H_CAVITY, side, {U[0], U[1], U[2]}, 0, {0}});
+}
+
+int hlbm_wall_bounce_back(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_wall_bounce_back: NULL context");
+  return add_hook(c, HookOp{HLBM_HOOK_PRE_STREAM, H_WALL_BB, 0, {0, 0, 0}, 0, {0}});
+}
+
+static bool post_hook(int32_t hook) {
+  return hook == HLBM_HOOK_POST_STREAM || hook == HLBM_HOOK_BOUNDARY_CONDITIONS;
+}
+
+int hlbm_post_bounce_back(hlbm_ctx* c, int32_t hook) {
+  if (!c || !post_hook(hook)) return fail(HLBM_EINVAL, "hlbm_post_bounce_back: hook must be post_stream_bcs or boundary_conditions");
+  return add_hook(c, HookOp{hook, H_POST_BB, 0, {0, 0, 0}, 0, {0}});
+}
+
+static int plane_hooks(hlbm_ctx* c, int32_t hook, int kind, const double U[3], const int32_t* regions, int32_t nreg,
+                       const char* name) {
+  if (!c || !U || !regions || nreg < 0 || !post_hook(hook))
+    return fail(HLBM_EINVAL, std::string(name) + ": bad argument");
+  for (int i = 0; i < nreg; i++) {  // check_traversal_allowed (grid_region.hpp:381-387)
+    if (regions[i] < 0 || regions[i] > 5) return fail(HLBM_EINVAL, std::string(name) + ": Traversal name not allowed");
+    add_hook(c, HookOp{hook, kind, regions[i], {U[0], U[1], U[2]}, 0, {0}});
+  }
+  return HLBM_OK;
+}
+
+int hlbm_neumann(hlbm_ctx* c, int32_t hook, const double U[3], const int32_t* regions, int32_t nregions) {
+  return plane_hooks(c, hook, H_NEUMANN, U, regions, nregions, "hlbm_neumann");
+}
+
+int hlbm_lid_driven_cavity(hlbm_ctx* c, int32_t hook, const double U[3], const int32_t* regions, int32_t nregions) {
+  return plane_hooks(c, hook, H_LID, U, regions, nregions, "hlbm_lid_driven_cavity");
+}
+
+int hlbm_start_set_distribution(hlbm_ctx* c, double value, const double bounds6[6]) {
+  if (!c || !bounds6) return fail(HLBM_EINVAL, "hlbm_start_set_distribution: bounds are required");
+  HookOp h{HLBM_HOOK_START_ITERATION, H_SETDIST, 0, {0, 0, 0}, value, {0}};
+  std::memcpy(h.bounds, bounds6, sizeof(h.bounds));
+  return add_hook(c, h);
+}
+
+int hlbm_step(hlbm_ctx* c, int64_t nsteps) {
+  if (!c || nsteps < 0) return fail(HLBM_EINVAL, "hlbm_step: bad argument");
+  if (nsteps == 0) return HLBM_OK;
+  if (int rc = set_device(c)) return rc;
+  if (int rc = build_plan(c)) return rc;
+  if (c->phase == MATER) c->phase = POSTCOL;
+  if (c->phase == RAW) {
+    HLBM_CK(launch_step_kernel(c, MODE_PROLOGUE, c->f[c->cur], c->f[1 - c->cur]));
+    c->cur = 1 - c->cur;
+    c->phase = POSTCOL;
+    c->steps++;
+    nsteps--;
+  }
+  for (int64_t s = 0; s < nsteps; s++) {
+    HLBM_CK(launch_step_kernel(c, MODE_FUSED, c->f[c->cur], c->f[1 - c->cur]));
+    c->cur = 1 - c->cur;
+    c->steps++;
+  }
+  return HLBM_OK;
+}
+
+int hlbm_sync(hlbm_ctx* c) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_sync: NULL context");
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_macro_variables(hlbm_ctx* c, double* rho, double* u) {
+  if (!c) return fail(HLBM_EINVAL, "hlbm_macro_variables: NULL context");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  double *drho = nullptr, *du = nullptr;
+  const size_t n = size_t(c->ncell);
+  if (rho && cudaMalloc(&drho, n * 8) != cudaSuccess) return fail(HLBM_ENOMEM, "hlbm_macro_variables: no memory");
+  if (u && cudaMalloc(&du, 3 * n * 8) != cudaSuccess) {
+    cudaFree(drho);
+    return fail(HLBM_ENOMEM, "hlbm_macro_variables: no memory");
+  }
+  StepPlan p;
+  base_plan(c, p);
+  c->launches += 2;
+  cudaError_t e = launch_macro_stats(c->precision, s, c->flags, p, drho, du, c->partials, c->stats_dev, c->stream);
+  if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, drho, n * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && u) e = cudaMemcpyAsync(u, du, 3 * n * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(drho);
+  cudaFree(du);
+  if (e != cudaSuccess) return fail(HLBM_ECUDA, std::string("hlbm_macro_variables: ") + cudaGetErrorString(e));
+  return HLBM_OK;
+}
+
+int hlbm_simulation_state(hlbm_ctx* c, double out[3]) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_simulation_state: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  StepPlan p;
+  base_plan(c, p);
+  c->launches += 2;
+  HLBM_CK(launch_macro_stats(c->precision, s, c->flags, p, nullptr, nullptr, c->partials, c->stats_dev, c->stream));
+  HLBM_CK(cudaMemcpyAsync(out, c->stats_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_get_populations(hlbm_ctx* c, double* out) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_get_populations: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  const size_t n = size_t(c->ncell);
+  if (elem_size(c->precision) == 8) {
+    HLBM_CK(cudaMemcpy2DAsync(out, n * 8, s, size_t(c->stride) * 8, n * 8, Q, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    if (!c->plane_tmp && cudaMalloc(&c->plane_tmp, n * 8) != cudaSuccess)
+      return fail(HLBM_ENOMEM, "hlbm_get_populations: no memory");
+    StepPlan p;
+    base_plan(c, p);
+    for (int i = 0; i < Q; i++) {
+      c->launches++;
+      HLBM_CK(launch_decode(c->precision, s, c->plane_tmp, i, p, c->stream));
+      HLBM_CK(cudaMemcpyAsync(out + i * n, c->plane_tmp, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_put_populations(hlbm_ctx* c, const double* in) {
+  if (!c || !in) return fail(HLBM_EINVAL, "hlbm_put_populations: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  const size_t n = size_t(c->ncell);
+  c->phase = RAW;
+  if (elem_size(c->precision) == 8) {
+    HLBM_CK(cudaMemcpy2DAsync(c->f[c->cur], size_t(c->stride) * 8, in, n * 8, n * 8, Q, cudaMemcpyHostToDevice,
+                              c->stream));
+  } else {
+    if (!c->plane_tmp && cudaMalloc(&c->plane_tmp, n * 8) != cudaSuccess)
+      return fail(HLBM_ENOMEM, "hlbm_put_populations: no memory");
+    StepPlan p;
+    base_plan(c, p);
+    for (int i = 0; i < Q; i++) {
+      HLBM_CK(cudaMemcpyAsync(c->plane_tmp, in + i * n, n * 8, cudaMemcpyHostToDevice, c->stream));
+      c->launches++;
+      HLBM_CK(launch_encode(c->precision, c->f[c->cur], c->plane_tmp, i, p, c->stream));
+    }
+  }
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_get_flags(hlbm_ctx* c, int8_t* out) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_get_flags: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  HLBM_CK(cudaMemcpyAsync(out, c->flags, size_t(c->ncell), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_put_flags(hlbm_ctx* c, const int8_t* in) {
+  if (!c || !in) return fail(HLBM_EINVAL, "hlbm_put_flags: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  HLBM_CK(cudaMemcpyAsync(c->flags, in, size_t(c->ncell), cudaMemcpyHostToDevice, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_info(hlbm_ctx* c, int64_t info[8]) {
+  if (!c || !info) return fail(HLBM_EINVAL, "hlbm_info: NULL argument");
+  info[0] = c->n[0];
+  info[1] = c->n[1];
+  info[2] = c->n[2];
+  info[3] = c->precision;
+  info[4] = c->steps;
+  info[5] = c->launches;
+  info[6] = int64_t(elem_size(c->precision));
+  info[7] = c->device;
+  return HLBM_OK;
+}
+
+void* hlbm_stream(hlbm_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+}  // extern "C"

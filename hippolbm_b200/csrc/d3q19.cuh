@@ -1,0 +1,69 @@
+// d3q19.cuh -- D3Q19 lattice constants and the node-local operator algebra shared by the
+// step kernels.  Direction order, weights and opposites follow LBMScheme<19>
+// (scheme.hpp:47-69): direction 0 is rest; for odd i, i and i+1 are opposites.
+#pragma once
+#include <cstdint>
+
+namespace hlbm {
+
+constexpr int Q = 19;
+constexpr int8_t FLAG_FLUID = -1;  // FLUIDE_ (enum.hpp:59)
+constexpr int8_t FLAG_WALL = -2;   // WALL_   (enum.hpp:60)
+
+struct D3Q19 {
+  static constexpr int ex[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+  static constexpr int ey[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+  static constexpr int ez[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+  static constexpr int wden[Q] = {3, 18, 18, 18, 18, 18, 18, 36, 36, 36, 36, 36, 36, 36, 36, 36, 36, 36, 36};
+  static constexpr int opp(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+};
+
+// Plane bounce-back tables (bounce_back.hpp:65-140): the populations saved before
+// streaming (pre) and where they are written back after streaming (post), per face
+// x_0, x_l, y_0, y_l, z_0, z_l (bounce_back_manager.hpp:50-56 numbering).
+struct PlaneBB {
+  static constexpr int pre[6][5] = {{2, 10, 8, 12, 14}, {1, 9, 7, 11, 13}, {4, 8, 9, 16, 18},
+                                    {3, 7, 10, 15, 17}, {6, 13, 12, 17, 16}, {5, 14, 11, 18, 15}};
+  static constexpr int post[6][5] = {{1, 9, 7, 11, 13}, {2, 10, 8, 12, 14}, {3, 7, 10, 15, 17},
+                                     {4, 8, 9, 16, 18}, {5, 14, 11, 18, 15}, {6, 13, 12, 17, 16}};
+};
+
+// Step plan: the node-local form of the operator lists of one deck.
+enum OpKind : int32_t { OP_POST_BB = 0, OP_ZOUHE = 1, OP_LID = 2, OP_SETDIST = 3 };
+constexpr int MAX_PLANE_OPS = 16;
+constexpr int MAX_CAVITY = 4;
+constexpr int MAX_SETS = 8;
+
+struct PlaneOp {
+  int32_t kind;  // OP_POST_BB (all non-periodic faces), OP_ZOUHE / OP_LID (one face)
+  int32_t face;  // 0..5
+  double u[3];   // lattice units
+};
+
+struct SetBox {  // set_distribution over a clipped box, applied at start_iteration
+  int32_t lo[3], hi[3];
+  double value;
+};
+
+struct StepPlan {
+  int32_t nx, ny, nz;
+  int32_t periodic[3];
+  int64_t ncell;
+  int64_t stride;  // elements between direction planes (>= ncell, padded)
+  int32_t collision;  // 0 BGK, 1 MRT
+  int32_t walls;      // wall_bounce_back active
+  int32_t has_force;
+  int32_t nops;
+  int32_t nsets;
+  int32_t ncav[6];    // cavity coefficient sets per face (z faces only)
+  double tau, inv_tau;
+  double F[3];
+  double mrt[8];      // s_e, s_eps, s_q, s_pi, s_m, w_eps, w_epsj, w_xx
+  double cav[6][MAX_CAVITY][5];
+  double rho0;        // reference density of the deviation storage (f - w * rho0)
+  double scale, inv_scale;  // deviation storage scale
+  PlaneOp ops[MAX_PLANE_OPS];
+  SetBox sets[MAX_SETS];
+};
+
+}  // namespace hlbm

@@ -1,0 +1,55 @@
+// launch.cuh -- host-side launch of the step kernel for one (storage, compute) type.
+// Each precision tier is its own translation unit so that the strict FP64 tier can be
+// compiled without FMA contraction (--fmad=false) while the others use FMA.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lbm_step.cuh"
+
+namespace hlbm {
+
+// Geometry of a step launch: x along threadIdx.x (coalesced SoA rows), y on threadIdx.y,
+// z on blockIdx.z.  256 threads per block.
+inline void step_geometry(const StepPlan& p, dim3& grid, dim3& block) {
+  int bx = 128;
+  if (p.nx < 128) bx = ((p.nx + 31) / 32) * 32;
+  int by = 256 / bx;
+  block = dim3(bx, by, 1);
+  grid = dim3((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, p.nz);
+}
+
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS>
+cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
+  dim3 grid, block;
+  step_geometry(p, grid, block);
+  k_step<S, R, STRICT, MODE, WALLS, true>
+      <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
+  return cudaGetLastError();
+}
+
+template <typename S, typename R, bool STRICT>
+cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                        cudaStream_t s) {
+  if (mode == MODE_PROLOGUE)
+    return walls ? launch_one<S, R, STRICT, MODE_PROLOGUE, true>(fin, fout, flags, p, s)
+                 : launch_one<S, R, STRICT, MODE_PROLOGUE, false>(fin, fout, flags, p, s);
+  if (mode == MODE_FUSED)
+    return walls ? launch_one<S, R, STRICT, MODE_FUSED, true>(fin, fout, flags, p, s)
+                 : launch_one<S, R, STRICT, MODE_FUSED, false>(fin, fout, flags, p, s);
+  return walls ? launch_one<S, R, STRICT, MODE_FINISH, true>(fin, fout, flags, p, s)
+               : launch_one<S, R, STRICT, MODE_FINISH, false>(fin, fout, flags, p, s);
+}
+
+// one entry per precision tier (defined in step_*.cu)
+cudaError_t step_f64_strict(int mode, int walls, const void* fin, void* fout, const int8_t* flags,
+                            const StepPlan& p, cudaStream_t s);
+cudaError_t step_f64(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                     cudaStream_t s);
+cudaError_t step_f32(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                     cudaStream_t s);
+cudaError_t step_f16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                     cudaStream_t s);
+cudaError_t step_bf16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                      cudaStream_t s);
+
+}  // namespace hlbm

@@ -1,0 +1,517 @@
+// lbm_step.cuh -- the fused D3Q19 time-step kernel (one node per thread, pull scheme on
+// two lattices, SoA populations over the real box, one flag byte per node).
+//
+// One launch advances the stored post-collision state C_k to C_{k+1}:
+//
+//   pull-stream from C_k  (periodic wrap by index arithmetic; on-node bounce-back where
+//                          the source is outside a non-periodic face or is a wall)
+//   -> post_stream_bcs / boundary_conditions  (node-local plane operators, deck order)
+//   -> start_iteration set_distribution boxes
+//   -> macro variables -> BGK or MRT collision  -> store C_{k+1}.
+//
+// This is the reference step (config_compute_loop.msp:27-37) re-phased: the reference keeps
+// S_k = post-stream state and runs macro -> collide -> pre_stream_bcs -> streaming
+// (step1, update_ghost, step2; streaming.cu:68-118) -> post_stream_bcs -> boundary_conditions.
+// The swap streaming bounces populations back on the node when the neighbour is outside the
+// ext box (streaming.hpp:62-64); wall_bounce_back (bounce_back.hpp:160-185) makes a fluid
+// node's population pulled from a wall equal to its own post-collision opposite; the plane
+// pre/post bounce-back pair (bounce_back.hpp:60-156) re-writes those same on-node values,
+// plus the cavity_z_* increments (cavity.hpp:74-87).  All of them are node-local in a pull
+// formulation, so they fuse.  MODE_PROLOGUE (collide S_0 in place of a pull) and MODE_FINISH
+// (stream + BCs, no collision: yields S_k) complete the re-phasing.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "d3q19.cuh"
+
+namespace hlbm {
+
+enum StepMode : int { MODE_PROLOGUE = 0, MODE_FUSED = 1, MODE_FINISH = 2 };
+
+// ------------------------------------------------------------------ storage codecs
+// Populations are stored as S and computed in R.  Half-precision storage keeps the
+// deviation (f_i - w_i * rho0) * scale, so that the stored numbers are small and their
+// relative precision is spent on the part of f that varies.
+template <typename S, typename R>
+struct Codec;
+
+template <>
+struct Codec<double, double> {
+  template <int I>
+  __device__ static __forceinline__ double dec(double s, const StepPlan&) { return s; }
+  template <int I>
+  __device__ static __forceinline__ double enc(double v, const StepPlan&) { return v; }
+};
+template <>
+struct Codec<float, float> {
+  template <int I>
+  __device__ static __forceinline__ float dec(float s, const StepPlan&) { return s; }
+  template <int I>
+  __device__ static __forceinline__ float enc(float v, const StepPlan&) { return v; }
+};
+template <>
+struct Codec<__half, float> {
+  template <int I>
+  __device__ static __forceinline__ float dec(__half s, const StepPlan& p) {
+    constexpr float w = 1.0f / D3Q19::wden[I];
+    return fmaf(__half2float(s), (float)p.inv_scale, w * (float)p.rho0);
+  }
+  template <int I>
+  __device__ static __forceinline__ __half enc(float v, const StepPlan& p) {
+    constexpr float w = 1.0f / D3Q19::wden[I];
+    return __float2half_rn((v - w * (float)p.rho0) * (float)p.scale);
+  }
+};
+template <>
+struct Codec<__nv_bfloat16, float> {
+  template <int I>
+  __device__ static __forceinline__ float dec(__nv_bfloat16 s, const StepPlan& p) {
+    constexpr float w = 1.0f / D3Q19::wden[I];
+    return fmaf(__bfloat162float(s), (float)p.inv_scale, w * (float)p.rho0);
+  }
+  template <int I>
+  __device__ static __forceinline__ __nv_bfloat16 enc(float v, const StepPlan& p) {
+    constexpr float w = 1.0f / D3Q19::wden[I];
+    return __float2bfloat16_rn((v - w * (float)p.rho0) * (float)p.scale);
+  }
+};
+
+template <typename S>
+__device__ __forceinline__ S ld_stream(const S* p) {
+  return __ldg(p);
+}
+
+// ------------------------------------------------------------------ compile-time loops
+template <int I, int N>
+struct Unroll {
+  template <class F>
+  __device__ static __forceinline__ void run(F&& f) {
+    f.template operator()<I>();
+    Unroll<I + 1, N>::run(f);
+  }
+};
+template <int N>
+struct Unroll<N, N> {
+  template <class F>
+  __device__ static __forceinline__ void run(F&&) {}
+};
+
+template <typename R, int I>
+__device__ __forceinline__ constexpr R weight() {
+  return R(1.0) / R(D3Q19::wden[I]);
+}
+
+// sum_{axis} e_axis * a_axis over the non-zero components in x, y, z order: the value of the
+// reference's (ex * ax + ey * ay) + ez * az with integer ex (adding a signed zero leaves a
+// non-zero sum unchanged).
+template <int I, typename R>
+__device__ __forceinline__ R edot(R ax, R ay, R az) {
+  constexpr int cx = D3Q19::ex[I], cy = D3Q19::ey[I], cz = D3Q19::ez[I];
+  R acc = R(0);
+  bool first = true;
+  if (cx != 0) {
+    acc = cx > 0 ? ax : -ax;
+    first = false;
+  }
+  if (cy != 0) {
+    acc = first ? (cy > 0 ? ay : -ay) : (cy > 0 ? acc + ay : acc - ay);
+    first = false;
+  }
+  if (cz != 0) {
+    acc = first ? (cz > 0 ? az : -az) : (cz > 0 ? acc + az : acc - az);
+  }
+  return acc;
+}
+
+// ------------------------------------------------------------------ macro variables
+// macro_variables.hpp:56-69: rho = sum f (index order, from 0), u = sum f e / rho when
+// rho > 1e-14, no half-force shift.
+template <typename R, bool STRICT>
+__device__ __forceinline__ void macro(const R (&v)[Q], R& rho, R& ux, R& uy, R& uz) {
+  rho = v[0];
+#pragma unroll
+  for (int i = 1; i < Q; i++) rho = rho + v[i];
+  ux = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
+  uy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
+  uz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
+  if (rho > R(1.0e-14)) {
+    if (STRICT) {
+      ux = ux / rho;
+      uy = uy / rho;
+      uz = uz / rho;
+    } else {
+      const R inv = R(1) / rho;
+      ux *= inv;
+      uy *= inv;
+      uz *= inv;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ BGK (bgk.hpp:47-62)
+template <typename R, bool STRICT>
+__device__ __forceinline__ void bgk(R (&v)[Q], const StepPlan& p) {
+  R rho, ux, uy, uz;
+  macro<R, STRICT>(v, rho, ux, uy, uz);
+  const R u_squ = (ux * ux + uy * uy + uz * uz);
+  const R tau = R(p.tau), inv_tau = R(p.inv_tau);
+  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  const bool force = p.has_force != 0;
+  Unroll<0, Q>::run([&]<int I>() {
+    constexpr R w = weight<R, I>();
+    const R eu = edot<I, R>(ux, uy, uz);
+    const R feq = w * rho * (R(1.) + R(3.) * eu + R(4.5) * eu * eu - R(1.5) * u_squ);
+    if (STRICT) {
+      R d = (feq - v[I]) / tau;
+      if (force) d = d + R(3.) * rho * w * edot<I, R>(Fx, Fy, Fz);
+      v[I] = v[I] + d;
+    } else {
+      R d = (feq - v[I]) * inv_tau;
+      if (force) d += R(3.) * rho * w * edot<I, R>(Fx, Fy, Fz);
+      v[I] += d;
+    }
+  });
+}
+
+// ------------------------------------------------------------------ MRT (mrt.hpp:42-193)
+// Moment basis rows, d'Humieres D3Q19 in the reference's order; each moment sums its
+// populations in increasing index, the reference's term order.
+struct MrtTables {
+  static constexpr signed char M[19][19] = {
+      {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+      {-30, -11, -11, -11, -11, -11, -11, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8},
+      {12, -4, -4, -4, -4, -4, -4, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+      {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0},
+      {0, -4, 4, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0},
+      {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1},
+      {0, 0, 0, -4, 4, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1},
+      {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1},
+      {0, 0, 0, 0, 0, -4, 4, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1},
+      {0, 2, 2, -1, -1, -1, -1, 1, 1, 1, 1, 1, 1, 1, 1, -2, -2, -2, -2},
+      {0, -4, -4, 2, 2, 2, 2, 1, 1, 1, 1, 1, 1, 1, 1, -2, -2, -2, -2},
+      {0, 0, 0, 1, 1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1, 0, 0, 0, 0},
+      {0, 0, 0, -2, -2, 2, 2, 1, 1, 1, 1, -1, -1, -1, -1, 0, 0, 0, 0},
+      {0, 0, 0, 0, 0, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 0, 0, 0, 0},
+      {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, -1, -1},
+      {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0},
+      {0, 0, 0, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, -1, 1, 0, 0, 0, 0},
+      {0, 0, 0, 0, 0, 0, 0, -1, 1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1},
+      {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, 1, -1}};
+  // back-transform coefficients num/den (mrt.hpp:129-173), moments in M's row order
+  static constexpr short BN[19][19] = {
+      {1, -5, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, 1, -1, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, -1, 1, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, 0, 0, 1, -1, 0, 0, -1, 1, 1, -1, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, 0, 0, -1, 1, 0, 0, -1, 1, 1, -1, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, 0, 0, 0, 0, 0, 0},
+      {1, -11, -1, 0, 0, 0, 0, -1, 1, -1, 1, -1, 1, 0, 0, 0, 0, 0, 0},
+      {1, 4, 1, 1, 1, 1, 1, 0, 0, 1, 1, 1, 1, 1, 0, 0, 1, -1, 0},
+      {1, 4, 1, -1, -1, -1, -1, 0, 0, 1, 1, 1, 1, 1, 0, 0, -1, 1, 0},
+      {1, 4, 1, 1, 1, -1, -1, 0, 0, 1, 1, 1, 1, -1, 0, 0, 1, 1, 0},
+      {1, 4, 1, -1, -1, 1, 1, 0, 0, 1, 1, 1, 1, -1, 0, 0, -1, -1, 0},
+      {1, 4, 1, 1, 1, 0, 0, 1, 1, 1, 1, -1, -1, 0, 0, 1, -1, 0, 1},
+      {1, 4, 1, -1, -1, 0, 0, -1, -1, 1, 1, -1, -1, 0, 0, 1, 1, 0, -1},
+      {1, 4, 1, 1, 1, 0, 0, -1, -1, 1, 1, -1, -1, 0, 0, -1, -1, 0, -1},
+      {1, 4, 1, -1, -1, 0, 0, 1, 1, 1, 1, -1, -1, 0, 0, -1, 1, 0, 1},
+      {1, 4, 1, 0, 0, 1, 1, 1, 1, -1, -1, 0, 0, 0, 1, 0, 0, 1, -1},
+      {1, 4, 1, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0, 1, 0, 0, -1, 1},
+      {1, 4, 1, 0, 0, 1, 1, -1, -1, -1, -1, 0, 0, 0, -1, 0, 0, 1, 1},
+      {1, 4, 1, 0, 0, -1, -1, 1, 1, -1, -1, 0, 0, 0, -1, 0, 0, -1, -1}};
+  // denominators by (row group, moment)
+  static constexpr short BD_AXIS[19] = {19, 2394, 63, 10, 10, 10, 10, 10, 10, 18, 18, 12, 12, 1, 1, 1, 1, 1, 1};
+  static constexpr short BD_DIAG[19] = {19, 1197, 252, 10, 40, 10, 40, 10, 40, 36, 72, 12, 24, 4, 4, 4, 8, 8, 8};
+  static constexpr short BD_REST[19] = {19, 399, 21, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+};
+
+template <int I>
+__device__ __forceinline__ constexpr int mrt_den(int k) {
+  return I == 0 ? MrtTables::BD_REST[k]
+                : (I <= 6 ? (k == 9 || k == 10 ? (I <= 2 ? 18 : 36) : MrtTables::BD_AXIS[k])
+                          : (k == 9 ? (I >= 15 ? 18 : 36) : (k == 10 ? (I >= 15 ? 36 : 72) : MrtTables::BD_DIAG[k])));
+}
+
+template <typename R, bool STRICT>
+__device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
+  R m[19];
+  Unroll<0, 19>::run([&]<int K>() {
+    R acc = R(0);
+    bool first = true;
+    Unroll<0, Q>::run([&]<int I>() {
+      constexpr int c = MrtTables::M[K][I];
+      if (c != 0) {
+        const R term = (c == 1) ? v[I] : (c == -1 ? -v[I] : R(c) * v[I]);
+        acc = first ? term : acc + term;
+        first = false;
+      }
+    });
+    m[K] = acc;
+  });
+  const R rho = m[0], e = m[1], eps = m[2], jx = m[3], qx = m[4], jy = m[5], qy = m[6], jz = m[7], qz = m[8],
+          pxx3 = m[9], pixx3 = m[10], pww = m[11], piww = m[12], pxy = m[13], pyz = m[14], pxz = m[15],
+          mx = m[16], my = m[17], mz = m[18];
+  const R s9 = STRICT ? R(1) / R(p.tau) : R(p.inv_tau), s13 = s9;
+  const R s1 = R(p.mrt[0]), s2 = R(p.mrt[1]), s4 = R(p.mrt[2]), s10 = R(p.mrt[3]), s16 = R(p.mrt[4]);
+  const R weps = R(p.mrt[5]), wepsj = R(p.mrt[6]), wxx = R(p.mrt[7]);
+  const R rho0 = R(1.);
+  const R jx2 = jx * jx, jy2 = jy * jy, jz2 = jz * jz;
+  const R jj = (jx2 + jy2 + jz2);
+  // relaxation (mrt.hpp:103-126), rho0 = 1
+  const R e_eq = R(-11) * rho + R(19) / rho0 * jj;
+  const R eps_eq = weps * rho + wepsj / rho0 * jj;
+  const R pxx3_eq = R(1) / (rho0) * (R(2) * jx2 - (jy2 + jz2));
+  const R pww_eq = R(1) / rho0 * (jy2 - jz2);
+  const R pxy_eq = R(1) / rho0 * jx * jy;
+  const R pyz_eq = R(1) / rho0 * jy * jz;
+  const R pxz_eq = R(1) / rho0 * jx * jz;
+  R mo[19];
+  mo[0] = rho;
+  mo[1] = e - s1 * (e - e_eq);
+  mo[2] = eps - s2 * (eps - eps_eq);
+  mo[3] = jx;
+  mo[4] = qx - s4 * (qx + R(2.) / R(3.) * jx);
+  mo[5] = jy;
+  mo[6] = qy - s4 * (qy + R(2.) / R(3.) * jy);
+  mo[7] = jz;
+  mo[8] = qz - s4 * (qz + R(2.) / R(3.) * jz);
+  mo[9] = pxx3 - s9 * (pxx3 - pxx3_eq);
+  mo[10] = pixx3 - s10 * (pixx3 - wxx * pxx3_eq);
+  mo[11] = pww - s9 * (pww - pww_eq);
+  mo[12] = piww - s10 * (piww - wxx * pww_eq);
+  mo[13] = pxy - s13 * (pxy - pxy_eq);
+  mo[14] = pyz - s13 * (pyz - pyz_eq);
+  mo[15] = pxz - s13 * (pxz - pxz_eq);
+  mo[16] = mx - s16 * mx;
+  mo[17] = my - s16 * my;
+  mo[18] = mz - s16 * mz;
+  // back-transform (mrt.hpp:129-173) then the force term (mrt.hpp:181-191)
+  const bool force = p.has_force != 0;
+  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  Unroll<0, Q>::run([&]<int I>() {
+    R acc = R(0);
+    bool first = true;
+    Unroll<0, 19>::run([&]<int K>() {
+      constexpr int num = MrtTables::BN[I][K];
+      if (num != 0) {
+        constexpr R coef = R(num < 0 ? -num : num) / R(mrt_den<I>(K));
+        const R term = coef * mo[K];
+        if (first)
+          acc = num < 0 ? -term : term;
+        else
+          acc = num < 0 ? acc - term : acc + term;
+        first = false;
+      }
+    });
+    if (force) acc = acc + R(3.) * rho * weight<R, I>() * edot<I, R>(Fx, Fy, Fz);
+    v[I] = acc;
+  });
+}
+
+// ------------------------------------------------------------------ Zou/He planes
+// neumann_{x,y,z}_{0,l}<19> (neumann.hpp:27-258) as one table per face.
+struct ZouHeFace {
+  int axis, t1, t2, den_sign;
+  int tang[9];
+  int known[5];
+  int A1[3], B1[3], A2[3], B2[3];
+  int main_dst, main_src, main_sign;
+  int diag[4][6];  // dst, src, s_n, s_t, t (1|2), sign of n_t
+};
+struct ZouHeTables {
+  static constexpr ZouHeFace face[6] = {
+      {0, 1, 2, -1, {3, 4, 5, 6, 15, 17, 18, 16, 0}, {2, 10, 8, 14, 12}, {3, 15, 17}, {4, 18, 16}, {5, 18, 15},
+       {6, 17, 16}, 1, 2, 1, {{9, 10, 1, -1, 1, 1}, {7, 8, 1, 1, 1, -1}, {11, 12, 1, 1, 2, -1}, {13, 14, 1, -1, 2, 1}}},
+      {0, 1, 2, 1, {3, 4, 5, 6, 15, 17, 18, 16, 0}, {1, 7, 9, 11, 13}, {3, 15, 17}, {4, 18, 16}, {5, 18, 15},
+       {6, 17, 16}, 2, 1, -1,
+       {{10, 9, -1, 1, 1, -1}, {8, 7, -1, -1, 1, 1}, {12, 11, -1, -1, 2, 1}, {14, 13, -1, 1, 2, -1}}},
+      {1, 0, 2, -1, {1, 2, 5, 6, 11, 13, 14, 12, 0}, {4, 9, 8, 18, 16}, {1, 11, 13}, {2, 14, 12}, {5, 11, 14},
+       {6, 13, 12}, 3, 4, 1, {{7, 8, 1, 1, 1, -1}, {10, 9, 1, -1, 1, 1}, {15, 16, 1, 1, 2, -1}, {17, 18, 1, -1, 2, 1}}},
+      {1, 0, 2, 1, {1, 2, 5, 6, 11, 13, 14, 12, 0}, {3, 7, 10, 15, 17}, {1, 11, 13}, {2, 14, 12}, {5, 11, 14},
+       {6, 13, 12}, 4, 3, -1,
+       {{8, 7, -1, -1, 1, 1}, {9, 10, -1, 1, 1, -1}, {16, 15, -1, -1, 2, 1}, {18, 17, -1, 1, 2, -1}}},
+      {2, 0, 1, -1, {0, 1, 2, 3, 4, 7, 9, 10, 8}, {6, 13, 12, 17, 16}, {1, 7, 9}, {2, 10, 8}, {3, 7, 10},
+       {4, 9, 8}, 5, 6, 1, {{11, 12, 1, 1, 1, -1}, {14, 13, 1, -1, 1, 1}, {15, 16, 1, 1, 2, -1}, {18, 17, 1, -1, 2, 1}}},
+      {2, 0, 1, 1, {0, 1, 2, 3, 4, 7, 9, 10, 8}, {5, 11, 14, 15, 18}, {1, 7, 9}, {2, 10, 8}, {3, 7, 10},
+       {4, 9, 8}, 6, 5, -1,
+       {{13, 14, -1, 1, 1, -1}, {12, 11, -1, -1, 1, 1}, {17, 18, -1, 1, 2, -1}, {16, 15, -1, -1, 2, 1}}}};
+};
+
+template <int F, typename R>
+__device__ __forceinline__ void zouhe(R (&v)[Q], const double* U) {
+  constexpr ZouHeFace z = ZouHeTables::face[F];
+  const R un = R(U[z.axis]), ut1 = R(U[z.t1]), ut2 = R(U[z.t2]);
+  R ts = v[z.tang[0]];
+#pragma unroll
+  for (int k = 1; k < 9; k++) ts = ts + v[z.tang[k]];
+  R ks = v[z.known[0]];
+#pragma unroll
+  for (int k = 1; k < 5; k++) ks = ks + v[z.known[k]];
+  const R den = z.den_sign > 0 ? (R(1.) + un) : (R(1.) - un);
+  const R rho = (ts + R(2.) * ks) / den;
+  const R n1 = (R(1.) / R(2.)) * ((v[z.A1[0]] + v[z.A1[1]] + v[z.A1[2]]) - (v[z.B1[0]] + v[z.B1[1]] + v[z.B1[2]])) -
+               (R(1.) / R(3.)) * rho * ut1;
+  const R n2 = (R(1.) / R(2.)) * ((v[z.A2[0]] + v[z.A2[1]] + v[z.A2[2]]) - (v[z.B2[0]] + v[z.B2[1]] + v[z.B2[2]])) -
+               (R(1.) / R(3.)) * rho * ut2;
+  const R mterm = (R(1.) / R(3.)) * rho * un;
+  v[z.main_dst] = z.main_sign > 0 ? v[z.main_src] + mterm : v[z.main_src] - mterm;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const R ut = z.diag[k][4] == 1 ? ut1 : ut2;
+    const R nt = z.diag[k][4] == 1 ? n1 : n2;
+    const R a = z.diag[k][2] > 0 ? un : -un;
+    const R comb = z.diag[k][3] > 0 ? a + ut : a - ut;
+    const R val = v[z.diag[k][1]] + (R(1.) / R(6.)) * rho * comb;
+    v[z.diag[k][0]] = z.diag[k][5] > 0 ? val + nt : val - nt;
+  }
+}
+
+// lid_driven_cavity (lid_driven_cavity.hpp:49-61): f = feq(sum f, U)
+template <typename R>
+__device__ __forceinline__ void lid(R (&v)[Q], const double* U) {
+  R rho = v[0];
+#pragma unroll
+  for (int i = 1; i < Q; i++) rho = rho + v[i];
+  const R Ux = R(U[0]), Uy = R(U[1]), Uz = R(U[2]);
+  const R u_squ = Ux * Ux + Uy * Uy + Uz * Uz;
+  Unroll<0, Q>::run([&]<int I>() {
+    const R eu = edot<I, R>(Ux, Uy, Uz);
+    v[I] = weight<R, I>() * rho * (R(1.) + R(3.) * eu + R(4.5) * eu * eu - R(1.5) * u_squ);
+  });
+}
+
+template <int F>
+__device__ __forceinline__ bool on_face(int x, int y, int z, const StepPlan& p) {
+  if (F == 0) return x == 0;
+  if (F == 1) return x == p.nx - 1;
+  if (F == 2) return y == 0;
+  if (F == 3) return y == p.ny - 1;
+  if (F == 4) return z == 0;
+  return z == p.nz - 1;
+}
+
+// post_bounce_back over the non-periodic faces in launcher order x0, xl, y0, yl, z0, zl
+// (post_bounce_back.cu:115-120): the value saved by pre_bounce_back is this node's own
+// post-collision opposite population, plus the cavity increments of that face.
+template <typename S, typename R>
+__device__ __forceinline__ void post_bb(R (&v)[Q], const S* __restrict__ fin, int64_t idx, int x, int y, int z,
+                                        const StepPlan& p) {
+  Unroll<0, 6>::run([&]<int F>() {
+    if (p.periodic[F / 2]) return;
+    if (!on_face<F>(x, y, z, p)) return;
+    Unroll<0, 5>::run([&]<int K>() {
+      constexpr int dst = PlaneBB::post[F][K], src = PlaneBB::pre[F][K];
+      R val = Codec<S, R>::template dec<src>(ld_stream(fin + src * p.stride + idx), p);
+      for (int c = 0; c < p.ncav[F]; c++) val = val + R(p.cav[F][c][K]);
+      v[dst] = val;
+    });
+  });
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, int64_t idx, int x, int y, int z,
+                                          int8_t flag, const StepPlan& p) {
+  for (int o = 0; o < p.nops; o++) {
+    const PlaneOp& op = p.ops[o];
+    if (op.kind == OP_POST_BB) {
+      post_bb<S, R>(v, fin, idx, x, y, z, p);
+      continue;
+    }
+    if (flag != FLAG_FLUID) continue;  // neuman / lid functors act on fluid nodes only
+    bool hit;
+    switch (op.face) {
+      case 0: hit = on_face<0>(x, y, z, p); break;
+      case 1: hit = on_face<1>(x, y, z, p); break;
+      case 2: hit = on_face<2>(x, y, z, p); break;
+      case 3: hit = on_face<3>(x, y, z, p); break;
+      case 4: hit = on_face<4>(x, y, z, p); break;
+      default: hit = on_face<5>(x, y, z, p); break;
+    }
+    if (!hit) continue;
+    if (op.kind == OP_LID) {
+      lid<R>(v, op.u);
+    } else {
+      switch (op.face) {
+        case 0: zouhe<0, R>(v, op.u); break;
+        case 1: zouhe<1, R>(v, op.u); break;
+        case 2: zouhe<2, R>(v, op.u); break;
+        case 3: zouhe<3, R>(v, op.u); break;
+        case 4: zouhe<4, R>(v, op.u); break;
+        default: zouhe<5, R>(v, op.u); break;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ the step kernel
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, bool PLANES>
+__global__ void __launch_bounds__(256, 1) k_step(const S* __restrict__ fin, S* __restrict__ fout,
+                                              const int8_t* __restrict__ flags, const StepPlan p) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= p.nx || y >= p.ny) return;
+  const int64_t idx = ((int64_t)z * p.ny + y) * p.nx + x;
+  const int8_t flag = flags[idx];
+  if (WALLS && flag == FLAG_WALL) {
+    if (MODE == MODE_FINISH)
+      Unroll<0, Q>::run([&]<int I>() { fout[I * p.stride + idx] = Codec<S, R>::template enc<I>(R(0), p); });
+    return;
+  }
+  R v[Q];
+  if (MODE == MODE_PROLOGUE) {
+    Unroll<0, Q>::run([&]<int I>() { v[I] = Codec<S, R>::template dec<I>(ld_stream(fin + I * p.stride + idx), p); });
+  } else {
+    // source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others flag "outside"
+    int sx[3], sy[3], sz[3];
+    bool ox[3], oy[3], oz[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int d = 1 - k;  // component of e_i: +1, 0, -1 -> source offset -d
+      int cx = x - d, cy = y - d, cz = z - d;
+      ox[k] = oy[k] = oz[k] = false;
+      if (cx < 0 || cx >= p.nx) {
+        if (p.periodic[0]) cx = cx < 0 ? cx + p.nx : cx - p.nx; else ox[k] = true;
+      }
+      if (cy < 0 || cy >= p.ny) {
+        if (p.periodic[1]) cy = cy < 0 ? cy + p.ny : cy - p.ny; else oy[k] = true;
+      }
+      if (cz < 0 || cz >= p.nz) {
+        if (p.periodic[2]) cz = cz < 0 ? cz + p.nz : cz - p.nz; else oz[k] = true;
+      }
+      sx[k] = cx;
+      sy[k] = cy;
+      sz[k] = cz;
+    }
+    Unroll<0, Q>::run([&]<int I>() {
+      constexpr int kx = 1 - D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
+      constexpr int O = D3Q19::opp(I);
+      bool bounce = ox[kx] || oy[ky] || oz[kz];
+      const int64_t src = ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx + sx[kx];
+      if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
+      const S* ptr = bounce ? fin + O * p.stride + idx : fin + I * p.stride + src;
+      const S raw = ld_stream(ptr);
+      v[I] = bounce ? Codec<S, R>::template dec<O>(raw, p) : Codec<S, R>::template dec<I>(raw, p);
+    });
+    if (PLANES) {
+      const bool boundary = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
+      if (boundary) plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
+    }
+  }
+  if (MODE != MODE_FINISH) {
+    for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
+      const SetBox& b = p.sets[s];
+      if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
+        Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
+    }
+    if (flag == FLAG_FLUID) {
+      if (p.collision == 0)
+        bgk<R, STRICT>(v, p);
+      else
+        mrt<R, STRICT>(v, p);
+    }
+  }
+  Unroll<0, Q>::run([&]<int I>() { fout[I * p.stride + idx] = Codec<S, R>::template enc<I>(v[I], p); });
+}
+
+}  // namespace hlbm

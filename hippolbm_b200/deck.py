@@ -83,6 +83,34 @@ class Case:
             setattr(c, k, v)
         return c
 
+    def to_dict(self) -> dict:
+        d = dataclasses.asdict(self)
+        for hook in HOOK_OPERATORS:
+            d[hook] = [[op.name, op.slots] for op in getattr(self, hook)]
+        return d
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Case":
+        d = dict(d)
+        for hook in HOOK_OPERATORS:
+            d[hook] = [Op(name, dict(slots)) for name, slots in d.get(hook, [])]
+        for k in ("cell_dims", "bmin", "bmax", "periodic", "Fext"):
+            d[k] = tuple(d[k])
+        if d.get("mrt_rates") is not None:
+            d["mrt_rates"] = tuple(d["mrt_rates"])
+        d["init_distributions"] = [(v, tuple(b) if b else None) for v, b in d.get("init_distributions", [])]
+        obs = []
+        for kind, oid, prm in d.get("obstacles", []):
+            if kind == "ball":
+                prm = (tuple(prm[0]), float(prm[1]))
+            elif kind == "wall":
+                prm = (tuple(prm[0]), tuple(prm[1]))
+            else:
+                prm = tuple(prm)
+            obs.append((kind, int(oid), prm))
+        d["obstacles"] = obs
+        return cls(**d)
+
     def validate(self) -> None:
         """Reject decks the reference rejects (domain_lbm.cpp:81-106) or the plan cannot hold."""
         n = self.nodes

@@ -1,0 +1,155 @@
+/*
+ * hippolbm.h -- C-ABI of the B200 D3Q19 lattice Boltzmann step.
+ *
+ * Each entry point stands in for one hippoLBM Onika operator on the time-step path (the
+ * operator's `execute()` is cited beside it).  A caller builds a lattice the way a deck's
+ * `initialize` list does (domain -> lbm_parameters -> set_distribution -> obstacles), records
+ * the compute-loop hooks in deck order (`pre_stream_bcs`, `post_stream_bcs`,
+ * `boundary_conditions`, `start_iteration`), then calls hlbm_step(), which runs whole
+ * compute_loop iterations (config_compute_loop.msp:27-37) as fused CUDA kernels.
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a negative HLBM_E* code on failure;
+ *     hlbm_last_error() returns the message of the calling thread's last failure.  The
+ *     library never exits the process (the reference prints and calls std::exit,
+ *     domain_lbm.cpp:85 and :105).
+ *   - A context is not thread-safe: callers serialise calls per context.  Each context owns
+ *     one CUDA stream; work is asynchronous on it unless the function copies to the host.
+ *   - Arrays are plain host pointers.  Populations are exchanged as FP64, SoA,
+ *     out[i * nz*ny*nx + (z*ny + y)*nx + x] over the real nodes (no ghost layers),
+ *     the reference's FieldView layout (field_view.hpp:56) without its 2 ghost layers.
+ *   - Velocities given to hlbm_neumann / hlbm_lid_driven_cavity are physical and are
+ *     divided by the celerity (convert_velocity<LBM_UNITS>, lbm_parameters.hpp:102-106);
+ *     cavity velocities are raw lattice values (cavity.cu:54,70), as in the reference.
+ */
+#ifndef HIPPOLBM_H
+#define HIPPOLBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hlbm_ctx hlbm_ctx;
+
+/* error codes */
+#define HLBM_OK 0
+#define HLBM_EINVAL (-1)   /* bad argument */
+#define HLBM_EDOMAIN (-2)  /* inconsistent domain (domain_lbm.cpp:81-106) */
+#define HLBM_ECUDA (-3)    /* CUDA runtime failure */
+#define HLBM_ENOMEM (-4)   /* device allocation failed */
+#define HLBM_EPLAN (-5)    /* operator list the fused step cannot express */
+#define HLBM_ESTATE (-6)   /* call not valid in the current state */
+
+/* precision tiers */
+#define HLBM_F64 0        /* FP64 storage and compute, FMA + reciprocal multiplies */
+#define HLBM_F64_STRICT 1 /* FP64, reference operation order, no FMA contraction */
+#define HLBM_F32 2        /* FP32 storage and compute */
+#define HLBM_F16 3        /* FP32 compute, FP16 storage of (f_i - w_i rho0) * scale */
+#define HLBM_BF16 4       /* FP32 compute, BF16 storage of (f_i - w_i rho0) * scale */
+
+/* compute-loop hooks (config_compute_loop.msp:7-21) */
+#define HLBM_HOOK_START_ITERATION 0
+#define HLBM_HOOK_PRE_STREAM 1
+#define HLBM_HOOK_POST_STREAM 2
+#define HLBM_HOOK_BOUNDARY_CONDITIONS 3
+
+/* plane regions, traversal names of grid_region.hpp:360-373 */
+#define HLBM_PLAN_YZ_0 0
+#define HLBM_PLAN_YZ_L 1
+#define HLBM_PLAN_XZ_0 2
+#define HLBM_PLAN_XZ_L 3
+#define HLBM_PLAN_XY_0 4
+#define HLBM_PLAN_XY_L 5
+
+const char* hlbm_last_error(void);
+/* Library version string. */
+const char* hlbm_version(void);
+
+/* domain (domain_lbm.cpp:66-110) followed by define_grid_3dq19 (define_lbm_fields.cpp:58-86),
+ * build_traversal (grid_region.hpp:89-197), init_obst (init_obst.hpp:29-32) and the default
+ * set_distribution of value 1 over the lattice (config_initialize.msp:22-23).  Nodes per axis
+ * = cell_dims + 1; dx = (bmax - bmin) / cell_dims must agree on all axes.  `device` selects the
+ * CUDA device.  On success *out owns device memory until hlbm_destroy(). */
+int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],
+                int32_t precision, int32_t device, hlbm_ctx** out);
+int hlbm_destroy(hlbm_ctx* ctx);
+
+/* lbm_parameters (lbm_parameters.cpp:73-99): tau if has_tau, else dt if dt > 0, else the
+ * celerity defines the lattice time step; Fext is converted to lattice units. */
+int hlbm_lbm_parameters(hlbm_ctx* ctx, const double Fext[3], double celerity, double nuth, double avg_rho,
+                        int32_t has_tau, double tau, double dt);
+/* out = {Fext_lb[3], celerity, dtLB, nuth, nu, tau, avg_rho} */
+int hlbm_get_parameters(hlbm_ctx* ctx, double out[9]);
+
+/* collision: bgk (bgk.cu:77-94) when kind == 0, mrt (mrt.cu:71-89) when kind == 1.
+ * rates8 = {s_e, s_eps, s_q, s_pi, s_m, w_eps, w_epsj, w_xx}; NULL keeps the reference's
+ * constants (mrt.hpp:43-47); s_nu = 1 / tau always. */
+int hlbm_collision(hlbm_ctx* ctx, int32_t kind, const double* rates8);
+
+/* Reduced-precision storage keeps (f_i - w_i * rho0) * scale (HLBM_F16: scale 1024 by
+ * default, HLBM_BF16: 1).  No reference counterpart: part of the precision tiers. */
+int hlbm_storage_scale(hlbm_ctx* ctx, double rho0, double scale);
+
+/* set_distribution (set_distribution.cu:69-109), applied now: f_i = value * w_i on the
+ * nodes of the box {int(min/dx), int(max/dx)} clipped to the lattice, or on all nodes when
+ * bounds6 is NULL.  do_update is accepted for compatibility (there are no ghost layers). */
+int hlbm_set_distribution(hlbm_ctx* ctx, double value, const double* bounds6, int32_t do_update);
+
+/* obstacles: init_obstacles (init_obstacles.cpp), register_solid_ball
+ * (register_solid_ball.cpp), register_solid_wall (register_solid_wall.cpp), register_quadrics
+ * (register_quadrics.cpp:72-79, q = the transformed 4x4 matrix, row-major), and the rasteriser
+ * update_obstacles (update_obstacles.cu:106-119), which marks WALL_ (-2) in the flag bytes. */
+int hlbm_init_obstacles(hlbm_ctx* ctx);
+int hlbm_register_solid_ball(hlbm_ctx* ctx, int32_t id, const double center[3], double radius);
+int hlbm_register_solid_wall(hlbm_ctx* ctx, int32_t id, const double bmin[3], const double bmax[3]);
+int hlbm_register_quadric(hlbm_ctx* ctx, int32_t id, const double q[16]);
+int hlbm_update_obstacles(hlbm_ctx* ctx);
+
+/* Compute-loop hooks, recorded in call order and executed inside every hlbm_step().
+ * pre_bounce_back (pre_bounce_back.cu:89-118), cavity_z_0 / cavity_z_l (cavity.cu:66-88,
+ * side 0 / 1) and wall_bounce_back (wall_bounce_back.cu:58-73) belong to pre_stream_bcs;
+ * post_bounce_back (post_bounce_back.cu:101-123), neumann (neuman.cu:69-122) and
+ * lid_driven_cavity (lid_driven_cavity.cu:69-93) to post_stream_bcs or boundary_conditions
+ * (`hook`); set_distribution with bounds to start_iteration. */
+int hlbm_clear_hooks(hlbm_ctx* ctx);
+int hlbm_pre_bounce_back(hlbm_ctx* ctx);
+int hlbm_cavity(hlbm_ctx* ctx, int32_t side, const double U[3]);
+int hlbm_wall_bounce_back(hlbm_ctx* ctx);
+int hlbm_post_bounce_back(hlbm_ctx* ctx, int32_t hook);
+int hlbm_neumann(hlbm_ctx* ctx, int32_t hook, const double U[3], const int32_t* regions, int32_t nregions);
+int hlbm_lid_driven_cavity(hlbm_ctx* ctx, int32_t hook, const double U[3], const int32_t* regions,
+                           int32_t nregions);
+int hlbm_start_set_distribution(hlbm_ctx* ctx, double value, const double bounds6[6]);
+
+/* nsteps iterations of compute_loop: macro_variables -> collision -> pre_stream_bcs ->
+ * streaming (streaming.cu:68-118, asynchrone: false) -> post_stream_bcs ->
+ * boundary_conditions.  Asynchronous on the context stream. */
+int hlbm_step(hlbm_ctx* ctx, int64_t nsteps);
+int hlbm_sync(hlbm_ctx* ctx);
+
+/* macro_variables (macro_variables.cu:71-90) of the current state, copied to the host:
+ * rho[n] and u[3 * n] (SoA); walls get u = 0 and rho = 0.  Either pointer may be NULL. */
+int hlbm_macro_variables(hlbm_ctx* ctx, double* rho, double* u);
+/* simulation_state (simulation_state.cu:73-98): out = {sum rho, min |u|, max |u|} over the
+ * nodes, FP64 on the device. */
+int hlbm_simulation_state(hlbm_ctx* ctx, double out[3]);
+
+/* populations of the current state (FP64, layout above); put replaces them */
+int hlbm_get_populations(hlbm_ctx* ctx, double* out);
+int hlbm_put_populations(hlbm_ctx* ctx, const double* in);
+/* flag bytes: -1 fluid, -2 wall (enum.hpp:59-60) */
+int hlbm_get_flags(hlbm_ctx* ctx, int8_t* out);
+int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
+
+/* info = {nx, ny, nz, precision, steps done, kernel launches, bytes per population, device} */
+int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
+/* the context's cudaStream_t, as a pointer-sized handle */
+void* hlbm_stream(hlbm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPPOLBM_H */
