@@ -1,0 +1,129 @@
+"""GPU fused step vs the CPU oracle, through the C-ABI.
+
+Every golden case (regression decks + operator cases) runs on the GPU and on the oracle for
+the same number of steps.  Tolerances:
+  - flags: bit-exact against the reference rasteriser (golden SHA);
+  - HLBM_F64_STRICT (reference operation order, no FMA): populations equal in value on every
+    node that carries state (walls excluded when wall_bounce_back is active: their
+    populations are scratch in the reference's in-place swap);
+  - HLBM_F64 (FMA, reciprocal multiplies): |f_gpu - f_ref| <= 1e-12 * max|f_ref| per population.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from hippolbm_b200.deck import Case
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "golden.json")) as fh:
+    GOLD = json.load(fh)
+F64_RTOL = 1e-12
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def oracle_state(oracle_mod, case, steps):
+    lat = oracle_mod.OracleLattice(case, "port").initialize().step(steps)
+    f = lat.real(lat.f()).copy()
+    obst = lat.real(lat.obst()).copy()
+    lat.close()
+    return f, obst
+
+
+def carried_mask(case, obst):
+    walls_skipped = any(op.name == "wall_bounce_back" for op in case.pre_stream_bcs)
+    return (obst != -2) if walls_skipped else np.ones_like(obst, dtype=bool)
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_strict_f64_equals_oracle(name, oracle_mod):
+    from hippolbm_b200.lattice import Lattice
+
+    g = GOLD[name]
+    case = Case.from_dict(g["case"])
+    f_ref, obst = oracle_state(oracle_mod, case, case.steps)
+    with Lattice.from_case(case, "f64_strict") as lat:
+        lat.step(case.steps)
+        f = lat.populations()
+        flags = lat.flags()
+    assert sha(flags.astype(np.int32)) == g["sha_obst"]
+    m = carried_mask(case, obst)
+    bad = np.argwhere((f != f_ref)[:, m])
+    assert bad.size == 0, f"{len(bad)} populations differ; first (dir, node) {bad[:3]}"
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_fast_f64_within_1e12(name, oracle_mod):
+    from hippolbm_b200.lattice import Lattice
+
+    g = GOLD[name]
+    case = Case.from_dict(g["case"])
+    f_ref, obst = oracle_state(oracle_mod, case, case.steps)
+    with Lattice.from_case(case, "f64") as lat:
+        lat.step(case.steps)
+        f = lat.populations()
+    m = carried_mask(case, obst)
+    err = np.abs(f - f_ref)[:, m].max()
+    assert err <= F64_RTOL * np.abs(f_ref[:, m]).max(), err
+
+
+def test_phase_bookkeeping_split_steps(oracle_mod):
+    """step(a); read; step(b) equals step(a + b): the read-out kernel leaves the state intact."""
+    from hippolbm_b200.lattice import Lattice
+
+    case = Case.from_dict(GOLD["mixed_ops_18x14x12"]["case"])
+    f_ref, obst = oracle_state(oracle_mod, case, 30)
+    with Lattice.from_case(case, "f64_strict") as lat:
+        lat.step(7)
+        lat.populations()
+        lat.simulation_state()
+        lat.step(1)
+        lat.step(22)
+        f = lat.populations()
+    m = carried_mask(case, obst)
+    assert np.array_equal(f[:, m], f_ref[:, m])
+
+
+def test_simulation_state_matches_oracle(oracle_mod):
+    from hippolbm_b200.lattice import Lattice
+
+    case = Case.from_dict(GOLD["regression_lbm_cavite_wall"]["case"])
+    lat_o = oracle_mod.OracleLattice(case, "port").initialize().step(40)
+    lat_o.lib.orc_macro_variables(lat_o.h)
+    st_ref = lat_o.simulation_state()
+    with Lattice.from_case(case, "f64_strict") as lat:
+        lat.step(40)
+        st = lat.simulation_state()
+        rho, u = lat.macro()
+    assert st[0] == pytest.approx(st_ref[0], rel=1e-14)
+    assert st[1] == pytest.approx(st_ref[1], abs=1e-15)
+    assert st[2] == pytest.approx(st_ref[2], rel=1e-14)
+    m0 = lat_o.real(lat_o.m0())
+    fluid = lat_o.real(lat_o.obst()) != -2
+    assert np.array_equal(rho[fluid], m0[fluid])
+
+
+def test_put_get_roundtrip_and_restart(oracle_mod):
+    """Populations written through the C-ABI restart the run exactly (checkpoint / resume)."""
+    from hippolbm_b200.lattice import Lattice
+
+    case = Case.from_dict(GOLD["couette12_mrt_small"]["case"])
+    with Lattice.from_case(case, "f64_strict") as a:
+        a.step(20)
+        snap = a.populations()
+        a.step(30)
+        f_a = a.populations()
+    with Lattice.from_case(case, "f64_strict") as b:
+        b.put_populations(snap)
+        b.step(30)
+        f_b = b.populations()
+    assert np.array_equal(f_a, f_b)
+    z = np.load(os.path.join(GOLDEN, GOLD["couette12_mrt_small"]["npz"]))
+    assert np.array_equal(f_a, z["f"])
