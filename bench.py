@@ -238,9 +238,10 @@ def run_ours(a):
     e2e = None
     lat = Lattice.from_case(case, a.precision, device=local)
     init = torch.empty(19 * nodes, dtype=torch.float64, pin_memory=True)
-    q = lat.populations()
-    init.numpy()[:] = q.reshape(-1)
-    del q
+    w = [1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12  # rest equilibrium, rho = 1
+    iv = init.numpy().reshape(19, nodes)
+    for i in range(19):
+        iv[i] = w[i]
     stats = (C.c_double * 3)()
     L = lat.L
 

@@ -55,6 +55,7 @@ SIGNATURES = {
     "hlbm_get_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
     "hlbm_put_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
     "hlbm_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "hlbm_tune": (C.c_int, [_vp, C.c_int32]),
     "hlbm_stream": (_vp, [_vp]),
 }
 

@@ -82,6 +82,7 @@ struct hlbm_ctx {
   double* plane_tmp = nullptr;
   cudaStream_t stream = nullptr;
   int phase = RAW;
+  int variant = 1;  // 1: vectorised step kernel where eligible, 0: one node per thread
   int64_t steps = 0;
   int64_t launches = 0;
   int64_t ncell = 0, stride = 0;
@@ -206,11 +207,11 @@ cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fou
   const int walls = p.walls;
   c->launches++;
   switch (c->precision) {
-    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream);
-    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream);
-    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream);
-    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream);
-    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream);
+    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
+    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
+    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
+    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
+    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
   }
 }
 
@@ -692,6 +693,12 @@ int hlbm_info(hlbm_ctx* c, int64_t info[8]) {
   info[5] = c->launches;
   info[6] = int64_t(elem_size(c->precision));
   info[7] = c->device;
+  return HLBM_OK;
+}
+
+int hlbm_tune(hlbm_ctx* c, int32_t variant) {
+  if (!c || variant < 0 || variant > 1) return fail(HLBM_EINVAL, "hlbm_tune: variant must be 0 or 1");
+  c->variant = variant;
   return HLBM_OK;
 }
 

@@ -4,7 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "lbm_step.cuh"
+#include "lbm_step_vec.cuh"
 
 namespace hlbm {
 
@@ -27,9 +27,47 @@ cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const S
   return cudaGetLastError();
 }
 
+// nodes per thread of the vectorised kernel: one 16-byte vector per direction plane
+template <typename S>
+constexpr int vec_npt() {
+  return sizeof(S) == 8 ? 2 : (sizeof(S) == 4 ? 4 : 8);
+}
+
+template <typename S>
+bool vec_eligible(const StepPlan& p, int walls) {
+  constexpr int NPT = vec_npt<S>();
+  return !walls && p.nx % NPT == 0 && p.nx / NPT >= 32;
+}
+
+inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, dim3& block) {
+  const int nvec = p.nx / npt;
+  int bx = block_x > 0 ? block_x : 128;
+  const int rounded = ((nvec + 31) / 32) * 32;
+  if (rounded < bx) bx = rounded;
+  const int by = 256 / bx > 0 ? 256 / bx : 1;
+  block = dim3(bx, by, 1);
+  grid = dim3((nvec + bx - 1) / bx, (p.ny + by - 1) / by, p.nz);
+}
+
+template <typename S, typename R, bool STRICT, int MODE>
+cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
+  constexpr int NPT = vec_npt<S>();
+  dim3 grid, block;
+  vec_geometry(p, NPT, 0, grid, block);
+  k_step_vec<S, R, STRICT, MODE, NPT>
+      <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
+  return cudaGetLastError();
+}
+
+// variant: 0 = one node per thread, 1 = vectorised when eligible
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                        cudaStream_t s) {
+                        cudaStream_t s, int variant) {
+  if (variant == 1 && vec_eligible<S>(p, walls)) {
+    if (mode == MODE_PROLOGUE) return launch_vec<S, R, STRICT, MODE_PROLOGUE>(fin, fout, flags, p, s);
+    if (mode == MODE_FUSED) return launch_vec<S, R, STRICT, MODE_FUSED>(fin, fout, flags, p, s);
+    return launch_vec<S, R, STRICT, MODE_FINISH>(fin, fout, flags, p, s);
+  }
   if (mode == MODE_PROLOGUE)
     return walls ? launch_one<S, R, STRICT, MODE_PROLOGUE, true>(fin, fout, flags, p, s)
                  : launch_one<S, R, STRICT, MODE_PROLOGUE, false>(fin, fout, flags, p, s);
@@ -42,14 +80,14 @@ cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const 
 
 // one entry per precision tier (defined in step_*.cu)
 cudaError_t step_f64_strict(int mode, int walls, const void* fin, void* fout, const int8_t* flags,
-                            const StepPlan& p, cudaStream_t s);
+                            const StepPlan& p, cudaStream_t s, int variant);
 cudaError_t step_f64(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s);
+                     cudaStream_t s, int variant);
 cudaError_t step_f32(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s);
+                     cudaStream_t s, int variant);
 cudaError_t step_f16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s);
+                     cudaStream_t s, int variant);
 cudaError_t step_bf16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                      cudaStream_t s);
+                      cudaStream_t s, int variant);
 
 }  // namespace hlbm

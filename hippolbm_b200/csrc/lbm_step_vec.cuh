@@ -1,0 +1,282 @@
+// lbm_step_vec.cuh -- the fused step with NPT consecutive x-nodes per thread.
+//
+// Same step as k_step (lbm_step.cuh), for lattices without wall obstacles: every direction
+// plane is read and written as one aligned vector per thread (double2, float4, or 8 packed
+// FP16/BF16 values: 16 bytes), which multiplies the bytes each thread keeps in flight by NPT.
+// A pull along e_x = +-1 needs the neighbouring element of the next/previous thread's vector:
+// it comes from a warp shuffle, and lanes at a warp edge fetch it with one scalar load (the
+// element of the previous/next warp, or the periodic image / on-node bounce-back at a row
+// end).  Warps never straddle rows: the x extent of a block is a multiple of 32 threads.
+#pragma once
+#include "lbm_step.cuh"
+
+namespace hlbm {
+
+// ------------------------------------------------------------------ vector chunks
+template <typename S, int NPT>
+struct Chunk;
+
+// plain element arrays for 8- and 4-byte types
+template <typename S, int NPT, typename V>
+struct ArrayChunk {
+  S e[NPT];
+  __device__ __forceinline__ void load(const S* p) {
+    const V v = __ldg(reinterpret_cast<const V*>(p));
+    static_assert(sizeof(V) == sizeof(S) * NPT, "vector width");
+    const S* s = reinterpret_cast<const S*>(&v);
+#pragma unroll
+    for (int k = 0; k < NPT; k++) e[k] = s[k];
+  }
+  __device__ __forceinline__ void store(S* p) const {
+    V v;
+    S* s = reinterpret_cast<S*>(&v);
+#pragma unroll
+    for (int k = 0; k < NPT; k++) s[k] = e[k];
+    *reinterpret_cast<V*>(p) = v;
+  }
+  template <int K>
+  __device__ __forceinline__ S get() const {
+    return e[K];
+  }
+  template <int K>
+  __device__ __forceinline__ void set(S v) {
+    e[K] = v;
+  }
+  __device__ __forceinline__ S first() const { return e[0]; }
+  __device__ __forceinline__ S last() const { return e[NPT - 1]; }
+  // [prev, e0 .. e_{NPT-2}]
+  __device__ __forceinline__ void shift_in_prev(S prev) {
+#pragma unroll
+    for (int k = NPT - 1; k > 0; k--) e[k] = e[k - 1];
+    e[0] = prev;
+  }
+  // [e1 .. e_{NPT-1}, next]
+  __device__ __forceinline__ void shift_in_next(S next) {
+#pragma unroll
+    for (int k = 0; k < NPT - 1; k++) e[k] = e[k + 1];
+    e[NPT - 1] = next;
+  }
+};
+
+template <>
+struct Chunk<double, 2> : ArrayChunk<double, 2, double2> {};
+template <>
+struct Chunk<float, 4> : ArrayChunk<float, 4, float4> {};
+template <>
+struct Chunk<float, 2> : ArrayChunk<float, 2, float2> {};
+
+// 16-bit types packed two per 32-bit word; element 2j is the low half of word j
+template <typename S, int NPT>
+struct PackedChunk {
+  static constexpr int W = NPT / 2;
+  unsigned w[W];
+  __device__ __forceinline__ void load(const S* p) {
+    if constexpr (W == 4) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+      w[0] = v.x;
+      w[1] = v.y;
+      w[2] = v.z;
+      w[3] = v.w;
+    } else {
+      const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+      w[0] = v.x;
+      w[1] = v.y;
+    }
+  }
+  __device__ __forceinline__ void store(S* p) const {
+    if constexpr (W == 4)
+      *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    else
+      *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+  }
+  static __device__ __forceinline__ S as_s(unsigned short b) {
+    S s;
+    memcpy(&s, &b, 2);
+    return s;
+  }
+  static __device__ __forceinline__ unsigned short bits(S s) {
+    unsigned short b;
+    memcpy(&b, &s, 2);
+    return b;
+  }
+  template <int K>
+  __device__ __forceinline__ S get() const {
+    return as_s((unsigned short)((K & 1) ? (w[K / 2] >> 16) : (w[K / 2] & 0xffffu)));
+  }
+  template <int K>
+  __device__ __forceinline__ void set(S v) {
+    const unsigned b = bits(v);
+    w[K / 2] = (K & 1) ? ((w[K / 2] & 0xffffu) | (b << 16)) : ((w[K / 2] & 0xffff0000u) | b);
+  }
+  __device__ __forceinline__ S first() const { return get<0>(); }
+  __device__ __forceinline__ S last() const { return get<NPT - 1>(); }
+  __device__ __forceinline__ void shift_in_prev(S prev) {
+    // new word j = (old element 2j-1 low, old element 2j high)
+#pragma unroll
+    for (int j = W - 1; j > 0; j--) w[j] = __byte_perm(w[j - 1], w[j], 0x5432);
+    w[0] = __byte_perm(unsigned(bits(prev)) << 16, w[0], 0x5432);
+  }
+  __device__ __forceinline__ void shift_in_next(S next) {
+    // new word j = (old element 2j+1 low, old element 2j+2 high)
+#pragma unroll
+    for (int j = 0; j < W - 1; j++) w[j] = __byte_perm(w[j], w[j + 1], 0x5432);
+    w[W - 1] = __byte_perm(w[W - 1], unsigned(bits(next)), 0x5432);
+  }
+};
+template <>
+struct Chunk<__half, 8> : PackedChunk<__half, 8> {};
+template <>
+struct Chunk<__half, 4> : PackedChunk<__half, 4> {};
+template <>
+struct Chunk<__nv_bfloat16, 8> : PackedChunk<__nv_bfloat16, 8> {};
+template <>
+struct Chunk<__nv_bfloat16, 4> : PackedChunk<__nv_bfloat16, 4> {};
+
+template <typename S>
+__device__ __forceinline__ S shfl_up1(S v) {
+  if constexpr (sizeof(S) == 2) {
+    unsigned short b;
+    memcpy(&b, &v, 2);
+    const unsigned r = __shfl_up_sync(0xffffffffu, unsigned(b), 1);
+    const unsigned short rb = (unsigned short)r;
+    S out;
+    memcpy(&out, &rb, 2);
+    return out;
+  } else {
+    return __shfl_up_sync(0xffffffffu, v, 1);
+  }
+}
+template <typename S>
+__device__ __forceinline__ S shfl_down1(S v) {
+  if constexpr (sizeof(S) == 2) {
+    unsigned short b;
+    memcpy(&b, &v, 2);
+    const unsigned r = __shfl_down_sync(0xffffffffu, unsigned(b), 1);
+    const unsigned short rb = (unsigned short)r;
+    S out;
+    memcpy(&out, &rb, 2);
+    return out;
+  } else {
+    return __shfl_down_sync(0xffffffffu, v, 1);
+  }
+}
+
+template <int NPT>
+__device__ __forceinline__ void load_flags(const int8_t* p, int8_t (&fl)[NPT]) {
+  if constexpr (NPT == 8) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+    const int8_t* b = reinterpret_cast<const int8_t*>(&v);
+#pragma unroll
+    for (int k = 0; k < 8; k++) fl[k] = b[k];
+  } else if constexpr (NPT == 4) {
+    const unsigned v = __ldg(reinterpret_cast<const unsigned*>(p));
+#pragma unroll
+    for (int k = 0; k < 4; k++) fl[k] = int8_t((v >> (8 * k)) & 0xff);
+  } else {
+    const unsigned short v = __ldg(reinterpret_cast<const unsigned short*>(p));
+    fl[0] = int8_t(v & 0xff);
+    fl[1] = int8_t(v >> 8);
+  }
+}
+
+// ------------------------------------------------------------------ the kernel
+template <typename S, typename R, bool STRICT, int MODE, int NPT>
+__global__ void __launch_bounds__(256, 1) k_step_vec(const S* __restrict__ fin, S* __restrict__ fout,
+                                                     const int8_t* __restrict__ flags, const StepPlan p) {
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;  // vector index along x
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const int nvec = p.nx / NPT;
+  const bool valid = tx < nvec && y < p.ny;  // invalid lanes still take part in the shuffles
+  const int lane = threadIdx.x & 31;
+  const int x0 = tx * NPT;
+  const int yy = y < p.ny ? y : p.ny - 1;
+  const int64_t row = ((int64_t)z * p.ny + yy) * p.nx;
+  Chunk<S, NPT> c[Q];
+  if (MODE == MODE_PROLOGUE) {
+    Unroll<0, Q>::run([&]<int I>() {
+      if (valid) c[I].load(fin + I * p.stride + row + x0);
+    });
+  } else {
+    int sy[3], sz[3];
+    bool oy[3], oz[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int d = 1 - k;
+      int cy = yy - d, cz = z - d;
+      oy[k] = oz[k] = false;
+      if (cy < 0 || cy >= p.ny) {
+        if (p.periodic[1]) cy = cy < 0 ? cy + p.ny : cy - p.ny; else oy[k] = true;
+      }
+      if (cz < 0 || cz >= p.nz) {
+        if (p.periodic[2]) cz = cz < 0 ? cz + p.nz : cz - p.nz; else oz[k] = true;
+      }
+      sy[k] = cy;
+      sz[k] = cz;
+    }
+    Unroll<0, Q>::run([&]<int I>() {
+      constexpr int ex = D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
+      constexpr int O = D3Q19::opp(I);
+      const bool row_out = oy[ky] || oz[kz];  // uniform over the warp
+      const S* own_opp = fin + O * p.stride + row + x0;
+      if (row_out) {  // every node of the vector bounces back on itself
+        if (valid) c[I].load(own_opp);
+        return;
+      }
+      const S* src = fin + I * p.stride + ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx;
+      if (valid) c[I].load(src + x0);
+      if constexpr (ex == 1) {  // node k pulls from x0 + k - 1
+        S prev = shfl_up1<S>(c[I].last());
+        if (lane == 0 && valid) {
+          if (x0 > 0)
+            prev = ld_stream(src + x0 - 1);
+          else if (p.periodic[0])
+            prev = ld_stream(src + p.nx - 1);
+          else
+            prev = ld_stream(own_opp);  // node 0 bounces back
+        }
+        c[I].shift_in_prev(prev);
+      } else if constexpr (ex == -1) {  // node k pulls from x0 + k + 1
+        S next = shfl_down1<S>(c[I].first());
+        const bool row_end = x0 + NPT >= p.nx;
+        if ((lane == 31 || row_end) && valid) {
+          if (!row_end)
+            next = ld_stream(src + x0 + NPT);
+          else if (p.periodic[0])
+            next = ld_stream(src);
+          else
+            next = ld_stream(own_opp + NPT - 1);  // node NPT-1 bounces back
+        }
+        c[I].shift_in_next(next);
+      }
+    });
+  }
+  if (!valid) return;
+  int8_t fl[NPT];
+  load_flags<NPT>(flags + row + x0, fl);
+  const bool yz_face = yy == 0 || z == 0 || yy == p.ny - 1 || z == p.nz - 1;
+  Unroll<0, NPT>::run([&]<int K>() {
+    const int x = x0 + K;
+    R v[Q];
+    Unroll<0, Q>::run([&]<int I>() { v[I] = Codec<S, R>::template dec<I>(c[I].template get<K>(), p); });
+    if (MODE != MODE_PROLOGUE && p.nops > 0 && (yz_face || x == 0 || x == p.nx - 1))
+      plane_ops<S, R>(v, fin, row + x, x, yy, z, fl[K], p);
+    if (MODE != MODE_FINISH) {
+      for (int s = 0; s < p.nsets; s++) {
+        const SetBox& b = p.sets[s];
+        if (x >= b.lo[0] && x <= b.hi[0] && yy >= b.lo[1] && yy <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
+          Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
+      }
+      if (fl[K] == FLAG_FLUID) {
+        if (p.collision == 0)
+          bgk<R, STRICT>(v, p);
+        else
+          mrt<R, STRICT>(v, p);
+      }
+    }
+    Unroll<0, Q>::run([&]<int I>() { c[I].template set<K>(Codec<S, R>::template enc<I>(v[I], p)); });
+  });
+  Unroll<0, Q>::run([&]<int I>() { c[I].store(fout + I * p.stride + row + x0); });
+}
+
+}  // namespace hlbm

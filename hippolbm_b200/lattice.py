@@ -160,5 +160,9 @@ class Lattice:
         keys = ["nx", "ny", "nz", "precision", "steps", "launches", "bytes_per_population", "device"]
         return dict(zip(keys, list(out)))
 
+    def tune(self, variant: int):
+        capi.check(self.L.hlbm_tune(self.h, int(variant)))
+        return self
+
     def stream_handle(self) -> int:
         return self.L.hlbm_stream(self.h) or 0

@@ -145,6 +145,10 @@ int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
 
 /* info = {nx, ny, nz, precision, steps done, kernel launches, bytes per population, device} */
 int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
+/* Step kernel selection (no reference counterpart): variant 1 (default) runs the vectorised
+ * kernel -- 16-byte vectors of consecutive x-nodes per thread -- when the lattice has no wall
+ * obstacles and nx splits into at least 32 vectors; variant 0 always runs one node per thread. */
+int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
 
