@@ -56,6 +56,7 @@ SIGNATURES = {
     "hlbm_put_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
     "hlbm_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "hlbm_tune": (C.c_int, [_vp, C.c_int32]),
+    "hlbm_autotune": (C.c_int, [_vp, C.c_int32, _i3, _d3]),
     "hlbm_stream": (_vp, [_vp]),
 }
 

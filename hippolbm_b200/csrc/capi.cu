@@ -82,7 +82,7 @@ struct hlbm_ctx {
   double* plane_tmp = nullptr;
   cudaStream_t stream = nullptr;
   int phase = RAW;
-  int variant = 1;  // 1: vectorised step kernel where eligible, 0: one node per thread
+  int variant = 0;  // step kernel variant (launch.cuh): kernel = variant % 2, occupancy = variant / 2
   int64_t steps = 0;
   int64_t launches = 0;
   int64_t ncell = 0, stride = 0;
@@ -202,17 +202,27 @@ int build_plan(hlbm_ctx* c) {
   return HLBM_OK;
 }
 
-cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fout) {
+cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fout, int variant) {
   const StepPlan& p = c->plan;
   const int walls = p.walls;
   c->launches++;
   switch (c->precision) {
-    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
-    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
-    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
-    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
-    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, c->variant);
+    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, variant);
+    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, variant);
+    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, variant);
+    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, variant);
+    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, variant);
   }
+}
+
+cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fout) {
+  return launch_step_variant(c, mode, fin, fout, c->variant);
+}
+
+// the vectorised kernel applies (launch.cuh: vec_eligible)
+bool vec_applies(const hlbm_ctx* c) {
+  const int npt = elem_size(c->precision) == 2 ? 4 : 2;
+  return !c->plan.walls && c->n[0] % npt == 0 && c->n[0] / npt >= 32;
 }
 
 // make S_k available; returns the buffer holding it
@@ -697,8 +707,51 @@ int hlbm_info(hlbm_ctx* c, int64_t info[8]) {
 }
 
 int hlbm_tune(hlbm_ctx* c, int32_t variant) {
-  if (!c || variant < 0 || variant > 1) return fail(HLBM_EINVAL, "hlbm_tune: variant must be 0 or 1");
+  if (!c || variant < 0 || variant >= NUM_VARIANTS)
+    return fail(HLBM_EINVAL, "hlbm_tune: variant must be in [0, " + std::to_string(NUM_VARIANTS) + ")");
   c->variant = variant;
+  return HLBM_OK;
+}
+
+int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_variant) {
+  if (!c || reps < 1) return fail(HLBM_EINVAL, "hlbm_autotune: bad argument");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = build_plan(c)) return rc;
+  // time fused launches from the current buffer into the idle one: the state does not advance
+  void* fin = c->f[c->cur];
+  void* fout = c->f[1 - c->cur];
+  if (c->phase == MATER) c->phase = POSTCOL;
+  cudaEvent_t e0, e1;
+  HLBM_CK(cudaEventCreate(&e0));
+  HLBM_CK(cudaEventCreate(&e1));
+  int best = c->variant;
+  float best_ms = 1e30f;
+  for (int v = 0; v < NUM_VARIANTS; v++) {
+    if (ms_per_variant) ms_per_variant[v] = -1.0;
+    if ((v % 2) == 1 && !vec_applies(c)) continue;
+    cudaError_t e = launch_step_variant(c, MODE_FUSED, fin, fout, v);  // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_step_variant(c, MODE_FUSED, fin, fout, v);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(HLBM_ECUDA, std::string("hlbm_autotune: ") + cudaGetErrorString(e));
+    }
+    ms /= reps;
+    if (ms_per_variant) ms_per_variant[v] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->variant = best;
+  if (chosen) *chosen = best;
   return HLBM_OK;
 }
 

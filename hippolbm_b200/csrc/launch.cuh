@@ -18,19 +18,20 @@ inline void step_geometry(const StepPlan& p, dim3& grid, dim3& block) {
   grid = dim3((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, p.nz);
 }
 
-template <typename S, typename R, bool STRICT, int MODE, bool WALLS>
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int MINB>
 cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
   dim3 grid, block;
   step_geometry(p, grid, block);
-  k_step<S, R, STRICT, MODE, WALLS, true>
+  k_step<S, R, STRICT, MODE, WALLS, true, MINB>
       <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
   return cudaGetLastError();
 }
 
-// nodes per thread of the vectorised kernel: one 16-byte vector per direction plane
+// nodes per thread of the vectorised kernel: one 8-byte vector per direction plane for the
+// 4- and 2-byte storage types (float2, 4 x FP16/BF16); FP64 uses double2
 template <typename S>
 constexpr int vec_npt() {
-  return sizeof(S) == 8 ? 2 : (sizeof(S) == 4 ? 4 : 8);
+  return sizeof(S) == 8 ? 2 : (sizeof(S) == 4 ? 2 : 4);
 }
 
 template <typename S>
@@ -49,33 +50,48 @@ inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, di
   grid = dim3((nvec + bx - 1) / bx, (p.ny + by - 1) / by, p.nz);
 }
 
-template <typename S, typename R, bool STRICT, int MODE>
+template <typename S, typename R, bool STRICT, int MODE, int MINB>
 cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
   constexpr int NPT = vec_npt<S>();
   dim3 grid, block;
   vec_geometry(p, NPT, 0, grid, block);
-  k_step_vec<S, R, STRICT, MODE, NPT>
+  k_step_vec<S, R, STRICT, MODE, NPT, MINB>
       <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
   return cudaGetLastError();
 }
 
-// variant: 0 = one node per thread, 1 = vectorised when eligible
+// Step kernel variants: variant % 2 selects the kernel (0: one node per thread, 1: vectorised
+// when eligible), variant / 2 the occupancy target: at least 1, 2 or 3 blocks of 256 threads per
+// SM (__launch_bounds__ minimum blocks, which caps registers at 255, 128 or 85 per thread).
+constexpr int NUM_VARIANTS = 6;
+
+template <typename S, typename R, bool STRICT, int MINB>
+cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fout, const int8_t* flags,
+                        const StepPlan& p, cudaStream_t s) {
+  if (vec) {
+    if (mode == MODE_PROLOGUE) return launch_vec<S, R, STRICT, MODE_PROLOGUE, MINB>(fin, fout, flags, p, s);
+    if (mode == MODE_FUSED) return launch_vec<S, R, STRICT, MODE_FUSED, MINB>(fin, fout, flags, p, s);
+    return launch_vec<S, R, STRICT, MODE_FINISH, MINB>(fin, fout, flags, p, s);
+  }
+  if (mode == MODE_PROLOGUE)
+    return walls ? launch_one<S, R, STRICT, MODE_PROLOGUE, true, MINB>(fin, fout, flags, p, s)
+                 : launch_one<S, R, STRICT, MODE_PROLOGUE, false, MINB>(fin, fout, flags, p, s);
+  if (mode == MODE_FUSED)
+    return walls ? launch_one<S, R, STRICT, MODE_FUSED, true, MINB>(fin, fout, flags, p, s)
+                 : launch_one<S, R, STRICT, MODE_FUSED, false, MINB>(fin, fout, flags, p, s);
+  return walls ? launch_one<S, R, STRICT, MODE_FINISH, true, MINB>(fin, fout, flags, p, s)
+               : launch_one<S, R, STRICT, MODE_FINISH, false, MINB>(fin, fout, flags, p, s);
+}
+
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
                         cudaStream_t s, int variant) {
-  if (variant == 1 && vec_eligible<S>(p, walls)) {
-    if (mode == MODE_PROLOGUE) return launch_vec<S, R, STRICT, MODE_PROLOGUE>(fin, fout, flags, p, s);
-    if (mode == MODE_FUSED) return launch_vec<S, R, STRICT, MODE_FUSED>(fin, fout, flags, p, s);
-    return launch_vec<S, R, STRICT, MODE_FINISH>(fin, fout, flags, p, s);
+  const bool vec = (variant % 2) == 1 && vec_eligible<S>(p, walls);
+  switch (variant / 2) {
+    case 0: return launch_minb<S, R, STRICT, 1>(mode, walls, vec, fin, fout, flags, p, s);
+    case 1: return launch_minb<S, R, STRICT, 2>(mode, walls, vec, fin, fout, flags, p, s);
+    default: return launch_minb<S, R, STRICT, 3>(mode, walls, vec, fin, fout, flags, p, s);
   }
-  if (mode == MODE_PROLOGUE)
-    return walls ? launch_one<S, R, STRICT, MODE_PROLOGUE, true>(fin, fout, flags, p, s)
-                 : launch_one<S, R, STRICT, MODE_PROLOGUE, false>(fin, fout, flags, p, s);
-  if (mode == MODE_FUSED)
-    return walls ? launch_one<S, R, STRICT, MODE_FUSED, true>(fin, fout, flags, p, s)
-                 : launch_one<S, R, STRICT, MODE_FUSED, false>(fin, fout, flags, p, s);
-  return walls ? launch_one<S, R, STRICT, MODE_FINISH, true>(fin, fout, flags, p, s)
-               : launch_one<S, R, STRICT, MODE_FINISH, false>(fin, fout, flags, p, s);
 }
 
 // one entry per precision tier (defined in step_*.cu)

@@ -444,8 +444,8 @@ __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, 
 }
 
 // ------------------------------------------------------------------ the step kernel
-template <typename S, typename R, bool STRICT, int MODE, bool WALLS, bool PLANES>
-__global__ void __launch_bounds__(256, 1) k_step(const S* __restrict__ fin, S* __restrict__ fout,
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, bool PLANES, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout,
                                               const int8_t* __restrict__ flags, const StepPlan p) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;

@@ -1,8 +1,9 @@
 // lbm_step_vec.cuh -- the fused step with NPT consecutive x-nodes per thread.
 //
 // Same step as k_step (lbm_step.cuh), for lattices without wall obstacles: every direction
-// plane is read and written as one aligned vector per thread (double2, float4, or 8 packed
-// FP16/BF16 values: 16 bytes), which multiplies the bytes each thread keeps in flight by NPT.
+// plane is read and written as one aligned vector per thread (double2, float2, or 4 packed
+// FP16/BF16 values), which multiplies the bytes each thread keeps in flight by NPT.  All loads
+// of a thread are issued before the first shuffle consumes one, so they overlap.
 // A pull along e_x = +-1 needs the neighbouring element of the next/previous thread's vector:
 // it comes from a warp shuffle, and lanes at a warp edge fetch it with one scalar load (the
 // element of the previous/next warp, or the periodic image / on-node bounce-back at a row
@@ -180,8 +181,8 @@ __device__ __forceinline__ void load_flags(const int8_t* p, int8_t (&fl)[NPT]) {
 }
 
 // ------------------------------------------------------------------ the kernel
-template <typename S, typename R, bool STRICT, int MODE, int NPT>
-__global__ void __launch_bounds__(256, 1) k_step_vec(const S* __restrict__ fin, S* __restrict__ fout,
+template <typename S, typename R, bool STRICT, int MODE, int NPT, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fin, S* __restrict__ fout,
                                                      const int8_t* __restrict__ flags, const StepPlan p) {
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;  // vector index along x
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -214,6 +215,10 @@ __global__ void __launch_bounds__(256, 1) k_step_vec(const S* __restrict__ fin, 
       sy[k] = cy;
       sz[k] = cz;
     }
+    // phase 1: issue every load (vectors, and the scalar edge elements of lanes at a warp or
+    // row edge) before any of them is consumed, so that they are all in flight together
+    const bool row_end = x0 + NPT >= p.nx;
+    S edge[Q];
     Unroll<0, Q>::run([&]<int I>() {
       constexpr int ex = D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
       constexpr int O = D3Q19::opp(I);
@@ -225,29 +230,31 @@ __global__ void __launch_bounds__(256, 1) k_step_vec(const S* __restrict__ fin, 
       }
       const S* src = fin + I * p.stride + ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx;
       if (valid) c[I].load(src + x0);
-      if constexpr (ex == 1) {  // node k pulls from x0 + k - 1
-        S prev = shfl_up1<S>(c[I].last());
-        if (lane == 0 && valid) {
-          if (x0 > 0)
-            prev = ld_stream(src + x0 - 1);
-          else if (p.periodic[0])
-            prev = ld_stream(src + p.nx - 1);
-          else
-            prev = ld_stream(own_opp);  // node 0 bounces back
+      if constexpr (ex == 1) {  // node 0 pulls from x0 - 1
+        if (lane == 0 && valid)
+          edge[I] = x0 > 0 ? ld_stream(src + x0 - 1)
+                           : (p.periodic[0] ? ld_stream(src + p.nx - 1) : ld_stream(own_opp));
+      } else if constexpr (ex == -1) {  // node NPT-1 pulls from x0 + NPT
+        if ((lane == 31 || row_end) && valid)
+          edge[I] = !row_end ? ld_stream(src + x0 + NPT)
+                             : (p.periodic[0] ? ld_stream(src) : ld_stream(own_opp + NPT - 1));
+      }
+    });
+    // phase 2: shift the x-pulled vectors by one node, taking the neighbour element from the
+    // adjacent lane (or from the edge load)
+    Unroll<0, Q>::run([&]<int I>() {
+      constexpr int ex = D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
+      if constexpr (ex != 0) {
+        if (oy[ky] || oz[kz]) return;
+        if constexpr (ex == 1) {
+          S prev = shfl_up1<S>(c[I].last());
+          if (lane == 0) prev = edge[I];
+          c[I].shift_in_prev(prev);
+        } else {
+          S next = shfl_down1<S>(c[I].first());
+          if (lane == 31 || row_end) next = edge[I];
+          c[I].shift_in_next(next);
         }
-        c[I].shift_in_prev(prev);
-      } else if constexpr (ex == -1) {  // node k pulls from x0 + k + 1
-        S next = shfl_down1<S>(c[I].first());
-        const bool row_end = x0 + NPT >= p.nx;
-        if ((lane == 31 || row_end) && valid) {
-          if (!row_end)
-            next = ld_stream(src + x0 + NPT);
-          else if (p.periodic[0])
-            next = ld_stream(src);
-          else
-            next = ld_stream(own_opp + NPT - 1);  // node NPT-1 bounces back
-        }
-        c[I].shift_in_next(next);
       }
     });
   }

@@ -164,5 +164,13 @@ class Lattice:
         capi.check(self.L.hlbm_tune(self.h, int(variant)))
         return self
 
+    def autotune(self, reps: int = 5):
+        """Time every step-kernel variant on this lattice (state unchanged) and keep the fastest;
+        returns (chosen variant, {variant: ms per step})."""
+        chosen = C.c_int32(0)
+        ms = (C.c_double * 6)()
+        capi.check(self.L.hlbm_autotune(self.h, int(reps), C.byref(chosen), ms))
+        return chosen.value, {v: ms[v] for v in range(6) if ms[v] >= 0}
+
     def stream_handle(self) -> int:
         return self.L.hlbm_stream(self.h) or 0

@@ -145,12 +145,19 @@ int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
 
 /* info = {nx, ny, nz, precision, steps done, kernel launches, bytes per population, device} */
 int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
-/* Step kernel selection (no reference counterpart): variant 1 (default) runs the vectorised
- * kernel -- 16-byte vectors of consecutive x-nodes per thread -- when the lattice has no wall
- * obstacles and nx splits into at least 32 vectors; variant 0 always runs one node per thread. */
+/* Step kernel selection (no reference counterpart).  variant % 2 picks the kernel: 0 = one node
+ * per thread, 1 = vectorised (consecutive x-nodes per thread in one vector per direction plane;
+ * used when the lattice has no wall obstacles and nx splits into >= 32 vectors, else the first
+ * kernel runs); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256 threads per SM.
+ * hlbm_autotune times `reps` fused launches of every variant on this lattice (from the current
+ * populations into the idle buffer, so the state does not advance), keeps the fastest, and
+ * returns it in *chosen and the per-variant times (ms, -1 if skipped) in ms_per_variant[6]. */
+#define HLBM_NUM_VARIANTS 6
 int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
+int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
+
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,9 @@
-"""The vectorised step kernel (NPT x-nodes per thread, 16-byte vectors, warp-shuffled x pulls)
-gives the same populations as the one-node-per-thread kernel, bit for bit, in every precision
-tier; in strict FP64 both equal the oracle.  Row lengths cover partial warps, several blocks per
-row, periodic x and bounce-back x ends."""
+"""The vectorised step kernel (NPT x-nodes per thread, vector loads, warp-shuffled x pulls) gives
+the same populations as the one-node-per-thread kernel.  Without FMA contraction (strict FP64)
+and after rounding to 16-bit storage the two agree bit for bit; the FMA tiers may contract a
+product differently in the two kernels, so FP64 agrees to 1e-12 and FP32 to 1e-6 of the
+largest population.  In strict FP64 both equal the oracle.  Row lengths cover partial warps,
+several blocks per row, periodic x and bounce-back x ends."""
 import numpy as np
 import pytest
 
@@ -9,7 +11,8 @@ from hippolbm_b200.deck import Case, Op
 
 pytestmark = pytest.mark.gpu
 
-NPT = {"f64": 2, "f64_strict": 2, "f32": 4, "f16": 8, "bf16": 8}
+NPT = {"f64": 2, "f64_strict": 2, "f32": 2, "f16": 4, "bf16": 4}
+RTOL = {"f64": 1e-12, "f64_strict": 0.0, "f32": 1e-6, "f16": 0.0, "bf16": 0.0}
 
 
 def case_for(nx, periodic_x, collision):
@@ -46,8 +49,9 @@ def test_vector_kernel_matches_scalar_kernel(precision, vectors, periodic_x):
         f0 = run(case, precision, 0)
         f1 = run(case, precision, 1)
         assert np.isfinite(f1).all()
-        diff = np.argwhere(f0 != f1)
-        assert diff.size == 0, f"{len(diff)} values differ, first {diff[:4]}"
+        tol = RTOL[precision] * np.abs(f0).max()
+        diff = np.argwhere(np.abs(f0 - f1) > tol)
+        assert diff.size == 0, f"{len(diff)} values differ beyond {tol}, first {diff[:4]}"
 
 
 @pytest.mark.parametrize("periodic_x", [True, False])
@@ -57,3 +61,31 @@ def test_vector_kernel_strict_equals_oracle(periodic_x, oracle_mod):
     f_ref = ref.real(ref.f()).copy()
     f = run(case, "f64_strict", 1)
     assert np.array_equal(f, f_ref)
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_every_variant_strict_equals_oracle(variant, oracle_mod):
+    """All six step-kernel variants (kernel x occupancy target) give the oracle's populations."""
+    from hippolbm_b200.lattice import Lattice
+
+    case = case_for(96, False, "bgk")
+    ref = oracle_mod.OracleLattice(case, "port").initialize().step(case.steps)
+    with Lattice.from_case(case, "f64_strict") as lat:
+        lat.tune(variant)
+        lat.step(case.steps)
+        assert np.array_equal(lat.populations(), ref.real(ref.f()))
+
+
+def test_autotune_keeps_the_state():
+    from hippolbm_b200.lattice import Lattice
+
+    case = case_for(128, True, "mrt")
+    with Lattice.from_case(case, "f64") as a, Lattice.from_case(case, "f64") as b:
+        a.step(7)
+        b.step(7)
+        chosen, times = a.autotune(reps=2)
+        assert chosen in times and all(t > 0 for t in times.values())
+        a.tune(0)
+        a.step(5)
+        b.step(5)
+        assert np.array_equal(a.populations(), b.populations())
