@@ -58,6 +58,7 @@ SIGNATURES = {
     "hlbm_tune": (C.c_int, [_vp, C.c_int32]),
     "hlbm_autotune": (C.c_int, [_vp, C.c_int32, _i3, _d3]),
     "hlbm_stream": (_vp, [_vp]),
+    "hlbm_simulation_state_static": (C.c_int, [_d3, C.c_int64, C.POINTER(C.c_int8), _i3, _d3, _vp]),
 }
 
 _lib = None

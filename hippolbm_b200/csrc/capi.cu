@@ -61,6 +61,11 @@ size_t elem_size(int prec) {
 constexpr double W_OF(int i) { return 1.0 / D3Q19::wden[i]; }
 }  // namespace
 
+namespace hlbm {
+// sets the message hlbm_last_error() returns, for entry points defined in other files
+int record_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace hlbm
+
 struct hlbm_ctx {
   int n[3];
   int periodic[3];

@@ -158,6 +158,20 @@ int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_v
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
 
+/* simulation_state for callers that cannot allocate device memory, such as an analysis hook
+ * inside a host application that owns the whole device budget, or a loop that must not pay
+ * cudaMalloc's device-wide synchronisation.  No counterpart in the reference.  The caller
+ * passes device pointers: FP64 populations f[i * stride + node] (stride >= node count), one
+ * flag byte per node, and out3 = {sum rho, min |u|, max |u|}; `stream` is a cudaStream_t or
+ * NULL; the call is asynchronous on it.  It allocates nothing: block partial sums go to a
+ * static __device__ array of HLBM_STATIC_PARTIALS slots (384 KiB held by every GPU that
+ * loads the library, until exit), so lattices above HLBM_STATIC_MAX_NODES nodes are rejected
+ * with HLBM_EINVAL.  The first call on a device looks up the array's address (make it before
+ * any stream capture).  All calls share the array: calls that overlap on the GPU race. */
+#define HLBM_STATIC_PARTIALS 16384
+#define HLBM_STATIC_MAX_NODES (16384LL * HLBM_STATIC_PARTIALS)
+int hlbm_simulation_state_static(const double* f, int64_t stride, const int8_t* flags, const int32_t n[3],
+                                 double* out3, void* stream);
 
 #ifdef __cplusplus
 }
