@@ -50,6 +50,9 @@ SIGNATURES = {
     "hlbm_sync": (C.c_int, [_vp]),
     "hlbm_macro_variables": (C.c_int, [_vp, _d3, _d3]),
     "hlbm_simulation_state": (C.c_int, [_vp, _d3]),
+    "hlbm_residual": (C.c_int, [_vp, _d3]),
+    "hlbm_moments": (C.c_int, [_vp, _d3]),
+    "hlbm_wall_force": (C.c_int, [_vp, _d3]),
     "hlbm_get_populations": (C.c_int, [_vp, _d3]),
     "hlbm_put_populations": (C.c_int, [_vp, _d3]),
     "hlbm_get_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
@@ -58,6 +61,13 @@ SIGNATURES = {
     "hlbm_tune": (C.c_int, [_vp, C.c_int32]),
     "hlbm_autotune": (C.c_int, [_vp, C.c_int32, _i3, _d3]),
     "hlbm_stream": (_vp, [_vp]),
+    "hlbm_batch_create": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "hlbm_batch_add": (C.c_int, [_vp, _vp]),
+    "hlbm_batch_remove": (C.c_int, [_vp, _vp]),
+    "hlbm_batch_step": (C.c_int, [_vp, C.c_int64]),
+    "hlbm_batch_tune": (C.c_int, [_vp, C.c_int32]),
+    "hlbm_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "hlbm_batch_destroy": (C.c_int, [_vp]),
     "hlbm_simulation_state_static": (C.c_int, [_d3, C.c_int64, C.POINTER(C.c_int8), _i3, _d3, _vp]),
 }
 

@@ -144,6 +144,116 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int npart
   }
 }
 
+// ------------------------------------------------------------------ sums over the lattice
+// Per-block FP64 partial sums of up to 4 quantities, folded by k_fold_sums in block order.
+template <int NS>
+__device__ __forceinline__ void block_sums(double (&acc)[NS], double* partials) {
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < NS; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], off);
+  __shared__ double sh[NS][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NS; k++) sh[k][warp] = acc[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      double a = sh[k][0];
+      for (int w = 1; w < int(blockDim.x >> 5); w++) a += sh[k][w];
+      partials[4 * blockIdx.x + k] = a;
+    }
+}
+
+__global__ void k_fold_sums(const double* __restrict__ partials, int nparts, double* __restrict__ out) {
+  __shared__ double sh[4][256];
+  double a[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 4; k++) a[k] += partials[4 * i + k];
+#pragma unroll
+  for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+#pragma unroll
+      for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = sh[k][0];
+}
+
+// steady-state residual: sum |u - u_prev|^2 and sum |u|^2 (FP64), then u_prev <- u (FP32 copy)
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_residual(const S* __restrict__ f, const int8_t* __restrict__ flags,
+                                                  int64_t ncell, float* __restrict__ uprev, int first,
+                                                  double* __restrict__ partials, const StepPlan p) {
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < ncell;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    if (flags[idx] < FLAG_FLUID) continue;
+    double v[Q], rho, ux, uy, uz;
+    Unroll<0, Q>::run([&]<int I>() { v[I] = double(Codec<S, R>::template dec<I>(f[I * p.stride + idx], p)); });
+    macro<double, true>(v, rho, ux, uy, uz);
+    const double px = uprev[idx], py = uprev[ncell + idx], pz = uprev[2 * ncell + idx];
+    if (!first) acc[0] += (ux - px) * (ux - px) + (uy - py) * (uy - py) + (uz - pz) * (uz - pz);
+    acc[1] += ux * ux + uy * uy + uz * uz;
+    uprev[idx] = float(ux);
+    uprev[ncell + idx] = float(uy);
+    uprev[2 * ncell + idx] = float(uz);
+  }
+  block_sums<4>(acc, partials);
+}
+
+// total mass and momentum: sum rho, sum rho u over fluid and passive nodes (FP64)
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_moments(const S* __restrict__ f, const int8_t* __restrict__ flags,
+                                                 int64_t ncell, double* __restrict__ partials, const StepPlan p) {
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < ncell;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    if (flags[idx] < FLAG_FLUID) continue;
+    double v[Q];
+    Unroll<0, Q>::run([&]<int I>() { v[I] = double(Codec<S, R>::template dec<I>(f[I * p.stride + idx], p)); });
+    double rho = v[0];
+    for (int i = 1; i < Q; i++) rho += v[i];
+    acc[0] += rho;
+    acc[1] += ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
+    acc[2] += ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
+    acc[3] += ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
+  }
+  block_sums<4>(acc, partials);
+}
+
+// Force on the walls by momentum exchange (no reference counterpart): for every fluid node x and
+// direction i whose neighbour x + e_i is a wall, the post-collision population f*_i(x) hits the
+// wall and comes back reversed, transferring 2 f*_i(x) e_i.  Reads the post-collision state.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_wall_force(const S* __restrict__ fpost, const int8_t* __restrict__ flags,
+                                                    double* __restrict__ partials, const StepPlan p) {
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < p.ncell;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    if (flags[idx] != FLAG_FLUID) continue;
+    const int x = int(idx % p.nx), y = int((idx / p.nx) % p.ny), z = int(idx / (int64_t(p.nx) * p.ny));
+    Unroll<1, Q>::run([&]<int I>() {
+      int xn = x + D3Q19::ex[I], yn = y + D3Q19::ey[I], zn = z + D3Q19::ez[I];
+      if (xn < 0 || xn >= p.nx) { if (!p.periodic[0]) return; xn = xn < 0 ? xn + p.nx : xn - p.nx; }
+      if (yn < 0 || yn >= p.ny) { if (!p.periodic[1]) return; yn = yn < 0 ? yn + p.ny : yn - p.ny; }
+      if (zn < 0 || zn >= p.nz) { if (!p.periodic[2]) return; zn = zn < 0 ? zn + p.nz : zn - p.nz; }
+      if (flags[(int64_t(zn) * p.ny + yn) * p.nx + xn] != FLAG_WALL) return;
+      const double fi = double(Codec<S, R>::template dec<I>(fpost[I * p.stride + idx], p));
+      acc[0] += 2.0 * fi * D3Q19::ex[I];
+      acc[1] += 2.0 * fi * D3Q19::ey[I];
+      acc[2] += 2.0 * fi * D3Q19::ez[I];
+    });
+  }
+  block_sums<4>(acc, partials);
+}
+
 // ------------------------------------------------------------------ FP64 <-> storage
 template <typename S, typename R, int I>
 __device__ __forceinline__ void dec_plane(const S* f, double* out, int64_t n, const StepPlan& p) {
@@ -220,6 +330,39 @@ cudaError_t launch_macro_stats(int prec, const void* f, const int8_t* flags, con
     case 3: return macro_stats_t<__half, float>(f, flags, p, rho, u, partials, out3, s);
     default: return macro_stats_t<__nv_bfloat16, float>(f, flags, p, rho, u, partials, out3, s);
   }
+}
+
+#define HLBM_PREC_DISPATCH(prec, CALL)                          \
+  switch (prec) {                                               \
+    case 2: { using S = float; using R = float; CALL; break; }  \
+    case 3: { using S = __half; using R = float; CALL; break; } \
+    case 4: { using S = __nv_bfloat16; using R = float; CALL; break; } \
+    default: { using S = double; using R = double; CALL; break; } \
+  }
+
+cudaError_t launch_residual(int prec, const void* f, const int8_t* flags, const StepPlan& p, float* uprev, int first,
+                            double* partials, double* out4, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  HLBM_PREC_DISPATCH(prec, (k_residual<S, R><<<nb, 256, 0, s>>>(static_cast<const S*>(f), flags, p.ncell, uprev,
+                                                                    first, partials, p)));
+  k_fold_sums<<<1, 256, 0, s>>>(partials, nb, out4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_moments(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* partials,
+                           double* out4, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  HLBM_PREC_DISPATCH(prec, (k_moments<S, R><<<nb, 256, 0, s>>>(static_cast<const S*>(f), flags, p.ncell, partials, p)));
+  k_fold_sums<<<1, 256, 0, s>>>(partials, nb, out4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wall_force(int prec, const void* fpost, const int8_t* flags, const StepPlan& p, double* partials,
+                              double* out4, cudaStream_t s) {
+  const int nb = stats_blocks(p.ncell);
+  HLBM_PREC_DISPATCH(prec, (k_wall_force<S, R><<<nb, 256, 0, s>>>(static_cast<const S*>(fpost), flags, partials, p)));
+  k_fold_sums<<<1, 256, 0, s>>>(partials, nb, out4);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s) {

@@ -21,6 +21,12 @@ cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], 
 int stats_blocks(int64_t ncell);
 cudaError_t launch_macro_stats(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* rho,
                                double* u, double* partials, double* out3, cudaStream_t s);
+cudaError_t launch_residual(int prec, const void* f, const int8_t* flags, const StepPlan& p, float* uprev, int first,
+                            double* partials, double* out4, cudaStream_t s);
+cudaError_t launch_moments(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* partials,
+                           double* out4, cudaStream_t s);
+cudaError_t launch_wall_force(int prec, const void* fpost, const int8_t* flags, const StepPlan& p, double* partials,
+                              double* out4, cudaStream_t s);
 cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s);
 cudaError_t launch_encode(int prec, void* f, const double* in, int dir, const StepPlan& p, cudaStream_t s);
 

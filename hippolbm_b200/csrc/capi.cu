@@ -10,6 +10,7 @@
 //           read-out (the next step overwrites it).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -85,6 +86,7 @@ struct hlbm_ctx {
   double* partials = nullptr;
   double* stats_dev = nullptr;
   double* plane_tmp = nullptr;
+  float* uprev = nullptr;  // velocity snapshot of hlbm_residual
   cudaStream_t stream = nullptr;
   int phase = RAW;
   int variant = 0;  // step kernel variant (launch.cuh): kernel = variant % 2, occupancy = variant / 2
@@ -93,6 +95,12 @@ struct hlbm_ctx {
   int64_t ncell = 0, stride = 0;
   StepPlan plan;
   bool plan_dirty = true;
+  // pipelined persistent kernel: plan and lattice descriptor in device memory, tile list
+  StepPlan* plan_dev = nullptr;
+  LatticeDesc* desc_dev = nullptr;
+  Tile* tiles_dev = nullptr;
+  int* err_dev = nullptr;
+  int ntiles = 0, tile_elems = 0, tma_stages = 0, tma_stages2 = 0, sms = 148;
 };
 
 namespace {
@@ -134,6 +142,64 @@ bool clip_box(const hlbm_ctx* c, const double mn[3], const double mx[3], int lo[
     hi[d] = hi[d] > c->n[d] - 1 ? c->n[d] - 1 : hi[d];
   }
   return true;
+}
+
+// Tiles of whole x-rows of about 512 nodes (256 in FP64); stages of one CTA per SM fit 226 KB of
+// shared memory, of two CTAs per SM 112 KB each; at least two stages are needed.
+bool pipeline_geometry(int nx, int ny, size_t es, int& rows, int& stages1, int& stages2) {
+  if ((size_t(nx) * es) % 16 != 0) return false;
+  const int target = es == 8 ? 256 : 512;
+  rows = target / nx;
+  rows = rows < 1 ? 1 : (rows > 32 ? 32 : rows);
+  if (rows > ny) rows = ny;
+  const size_t stage_bytes = size_t(Q) * rows * nx * es;
+  const size_t head = tma_head_bytes();
+  stages1 = int((226 * 1024 - head) / stage_bytes);
+  stages2 = int((112 * 1024 - head) / stage_bytes);
+  stages1 = stages1 > 4 ? 4 : stages1;
+  stages2 = stages2 > 4 ? 4 : stages2;
+  return stages1 >= 2;
+}
+
+// Tile list and stage geometry of the pipelined kernel (lbm_step_tma.cuh).
+int setup_pipeline(hlbm_ctx* c) {
+  const StepPlan& p = c->plan;
+  if (!c->plan_dev) {
+    if (cudaMalloc(&c->plan_dev, sizeof(StepPlan)) != cudaSuccess ||
+        cudaMalloc(&c->desc_dev, sizeof(LatticeDesc)) != cudaSuccess)
+      return fail(HLBM_ENOMEM, "cannot allocate the step plan");
+  }
+  HLBM_CK(cudaMemcpyAsync(c->plan_dev, &p, sizeof(StepPlan), cudaMemcpyHostToDevice, c->stream));
+  LatticeDesc d{};
+  d.plan = c->plan_dev;
+  d.f[0] = c->f[0];
+  d.f[1] = c->f[1];
+  d.flags = c->flags;
+  d.cur = 0;
+  HLBM_CK(cudaMemcpyAsync(c->desc_dev, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+  c->tma_stages = 0;
+  c->tma_stages2 = 0;
+  const size_t es = elem_size(c->precision);
+  int rows = 0, stages1 = 0, stages2 = 0;
+  if (!pipeline_geometry(p.nx, p.ny, es, rows, stages1, stages2)) return HLBM_OK;
+  const int tile_elems = rows * p.nx;
+  const int stages = stages1;
+  std::vector<Tile> tiles;
+  for (int z = 0; z < p.nz; z++)
+    for (int y0 = 0; y0 < p.ny; y0 += rows) tiles.push_back(make_int4(0, z, y0, (p.ny - y0) < rows ? (p.ny - y0) : rows));
+  if (int(tiles.size()) != c->ntiles) {
+    cudaFree(c->tiles_dev);
+    c->tiles_dev = nullptr;
+    if (cudaMalloc(&c->tiles_dev, tiles.size() * sizeof(Tile)) != cudaSuccess)
+      return fail(HLBM_ENOMEM, "cannot allocate the tile list");
+  }
+  HLBM_CK(cudaMemcpyAsync(c->tiles_dev, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  c->ntiles = int(tiles.size());
+  c->tile_elems = tile_elems;
+  c->tma_stages = stages;
+  c->tma_stages2 = stages2;
+  return HLBM_OK;
 }
 
 int build_plan(hlbm_ctx* c) {
@@ -203,6 +269,7 @@ int build_plan(hlbm_ctx* c) {
     }
     b.value = h.value;
   }
+  if (int rc = setup_pipeline(c)) return rc;
   c->plan_dirty = false;
   return HLBM_OK;
 }
@@ -210,14 +277,37 @@ int build_plan(hlbm_ctx* c) {
 cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fout, int variant) {
   const StepPlan& p = c->plan;
   const int walls = p.walls;
+  TmaArgs t;
+  t.desc = c->desc_dev;
+  t.tiles = c->tiles_dev;
+  t.ntiles = c->ntiles;
+  t.tile_elems = c->tile_elems;
+  // variant 6: two CTAs per SM when two CTAs' stages fit, variant 7: one CTA, deeper staging
+  t.ctas_per_sm = (variant == 6 && c->tma_stages2 >= 2) ? 2 : 1;
+  t.stages = t.ctas_per_sm == 2 ? c->tma_stages2 : c->tma_stages;
+  t.parity = (fin == c->f[0]) ? 0 : 1;
+  t.err = c->err_dev;
+  t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
   c->launches++;
   switch (c->precision) {
-    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, variant);
-    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, variant);
-    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, variant);
-    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, variant);
-    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, variant);
+    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
+    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
+    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
+    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
+    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
   }
+}
+
+// a pipelined-kernel wait that timed out leaves a code in the device error word
+int check_device_error(hlbm_ctx* c) {
+  int e = 0;
+  HLBM_CK(cudaMemcpyAsync(&e, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  if (e != 0) {
+    cudaMemsetAsync(c->err_dev, 0, sizeof(int), c->stream);
+    return fail(HLBM_ECUDA, "step kernel: a shared-memory pipeline wait timed out (error " + std::to_string(e) + ")");
+  }
+  return HLBM_OK;
 }
 
 cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fout) {
@@ -232,6 +322,7 @@ bool vec_applies(const hlbm_ctx* c) {
 
 // make S_k available; returns the buffer holding it
 int state_buffer(hlbm_ctx* c, void** out) {
+  if (int rc = check_device_error(c)) return rc;
   if (c->phase == RAW) {
     *out = c->f[c->cur];
     return HLBM_OK;
@@ -303,6 +394,9 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
   c->ncell = int64_t(n[0]) * n[1] * n[2];
   c->stride = (c->ncell + 127) / 128 * 128;
   if (precision == HLBM_F16) c->scale = 1024.0;
+  // default step-kernel variant per tier, from hlbm_autotune on 512^3 Couette (B200): FP64 one
+  // node per thread at >= 3 blocks/SM; FP32 vectorised at >= 3; FP16/BF16 vectorised at >= 2
+  c->variant = (precision == HLBM_F32) ? 5 : ((precision == HLBM_F16 || precision == HLBM_BF16) ? 3 : 4);
   mrt_reference(c->mrt);
   auto cleanup = [&](int rc) {
     hlbm_destroy(c);
@@ -318,8 +412,13 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
       return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate " + std::to_string(fbytes >> 20) +
                                            " MiB of populations"));
     }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc(&c->err_dev, sizeof(int)) != cudaSuccess || cudaMemsetAsync(c->err_dev, 0, sizeof(int), c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate the error word"));
+  }
   if (cudaMalloc(&c->flags, size_t(c->ncell)) != cudaSuccess ||
-      cudaMalloc(&c->partials, sizeof(double) * 3 * 148 * 8) != cudaSuccess ||
+      cudaMalloc(&c->partials, sizeof(double) * 4 * 148 * 8) != cudaSuccess ||
       cudaMalloc(&c->stats_dev, sizeof(double) * 4) != cudaSuccess) {
     cudaGetLastError();
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate flags"));
@@ -346,6 +445,11 @@ int hlbm_destroy(hlbm_ctx* c) {
   cudaFree(c->partials);
   cudaFree(c->stats_dev);
   cudaFree(c->plane_tmp);
+  cudaFree(c->uprev);
+  cudaFree(c->plan_dev);
+  cudaFree(c->desc_dev);
+  cudaFree(c->tiles_dev);
+  cudaFree(c->err_dev);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return HLBM_OK;
@@ -594,7 +698,7 @@ int hlbm_step(hlbm_ctx* c, int64_t nsteps) {
 int hlbm_sync(hlbm_ctx* c) {
   if (!c) return fail(HLBM_EINVAL, "hlbm_sync: NULL context");
   HLBM_CK(cudaStreamSynchronize(c->stream));
-  return HLBM_OK;
+  return check_device_error(c);
 }
 
 int hlbm_macro_variables(hlbm_ctx* c, double* rho, double* u) {
@@ -633,6 +737,60 @@ int hlbm_simulation_state(hlbm_ctx* c, double out[3]) {
   HLBM_CK(launch_macro_stats(c->precision, s, c->flags, p, nullptr, nullptr, c->partials, c->stats_dev, c->stream));
   HLBM_CK(cudaMemcpyAsync(out, c->stats_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_residual(hlbm_ctx* c, double* out) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_residual: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  int first = 0;
+  if (!c->uprev) {
+    if (cudaMalloc(&c->uprev, size_t(c->ncell) * 3 * sizeof(float)) != cudaSuccess)
+      return fail(HLBM_ENOMEM, "hlbm_residual: no memory for the velocity snapshot");
+    first = 1;
+  }
+  StepPlan p;
+  base_plan(c, p);
+  c->launches += 2;
+  double h[4];
+  HLBM_CK(launch_residual(c->precision, s, c->flags, p, c->uprev, first, c->partials, c->stats_dev, c->stream));
+  HLBM_CK(cudaMemcpyAsync(h, c->stats_dev, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  *out = first ? HUGE_VAL : (h[1] > 0 ? std::sqrt(h[0] / h[1]) : (h[0] > 0 ? HUGE_VAL : 0.0));
+  return HLBM_OK;
+}
+
+int hlbm_moments(hlbm_ctx* c, double out[4]) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_moments: NULL argument");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  StepPlan p;
+  base_plan(c, p);
+  c->launches += 2;
+  HLBM_CK(launch_moments(c->precision, s, c->flags, p, c->partials, c->stats_dev, c->stream));
+  HLBM_CK(cudaMemcpyAsync(out, c->stats_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_wall_force(hlbm_ctx* c, double out[3]) {
+  if (!c || !out) return fail(HLBM_EINVAL, "hlbm_wall_force: NULL argument");
+  if (c->phase == RAW) return fail(HLBM_ESTATE, "hlbm_wall_force: needs a post-collision state (step once first)");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = check_device_error(c)) return rc;
+  StepPlan p;
+  base_plan(c, p);
+  c->launches += 2;
+  double h[4];
+  HLBM_CK(launch_wall_force(c->precision, c->f[c->cur], c->flags, p, c->partials, c->stats_dev, c->stream));
+  HLBM_CK(cudaMemcpyAsync(h, c->stats_dev, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  out[0] = h[0];
+  out[1] = h[1];
+  out[2] = h[2];
   return HLBM_OK;
 }
 
@@ -733,7 +891,8 @@ int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_var
   float best_ms = 1e30f;
   for (int v = 0; v < NUM_VARIANTS; v++) {
     if (ms_per_variant) ms_per_variant[v] = -1.0;
-    if ((v % 2) == 1 && !vec_applies(c)) continue;
+    if (v < 6 && (v % 2) == 1 && !vec_applies(c)) continue;
+    if (v >= 6 && c->tma_stages < 2) continue;
     cudaError_t e = launch_step_variant(c, MODE_FUSED, fin, fout, v);  // warm-up
     if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
     for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_step_variant(c, MODE_FUSED, fin, fout, v);
@@ -755,11 +914,296 @@ int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_var
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (int rc = check_device_error(c)) return rc;
   c->variant = best;
   if (chosen) *chosen = best;
   return HLBM_OK;
 }
 
 void* hlbm_stream(hlbm_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Batches: many lattices, one pipelined persistent-kernel launch per time step.
+struct hlbm_batch {
+  int precision;
+  int device;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::vector<hlbm_ctx*> members;
+  bool dirty = true;
+  LatticeDesc* desc_dev = nullptr;
+  Tile* tiles_dev = nullptr;
+  size_t desc_cap = 0, tiles_cap = 0;
+  int ntiles = 0, tile_elems = 0, stages = 0, stages2 = 0, walls = 0;
+  int variant = 8;  // 8, 9: tile-list kernel (>= 3 or 2 CTAs per SM); 6, 7: pipelined kernel
+  bool descs_stale = true;
+  int* err_dev = nullptr;
+  cudaGraphExec_t graph = nullptr;  // two steps: parity 0 then parity 1
+  int64_t replays = 0, launches = 0;
+};
+
+namespace {
+
+int batch_fail(int code, const std::string& m) { return fail(code, m); }
+
+void batch_drop_graph(hlbm_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+// rebuild the concatenated tile list and the descriptors of the members
+int batch_rebuild(hlbm_batch* b) {
+  if (!b->dirty) return HLBM_OK;
+  batch_drop_graph(b);
+  const size_t es = elem_size(b->precision);
+  int tile_elems = 0, walls = 0;
+  std::vector<int> rows_of(b->members.size());
+  for (size_t m = 0; m < b->members.size(); m++) {
+    hlbm_ctx* c = b->members[m];
+    if (int rc = build_plan(c)) return rc;
+    int rows, s1, s2;
+    if (b->variant >= 8) {  // tile-list kernel: about 256 nodes (one per thread) per tile, any nx
+      rows = std::max(1, std::min(c->n[1], 256 / c->n[0]));
+    } else if (!pipeline_geometry(c->n[0], c->n[1], es, rows, s1, s2)) {
+      return batch_fail(HLBM_EPLAN, "pipelined batch: nx * bytes per population must be a multiple of 16");
+    }
+    rows_of[m] = rows;
+    tile_elems = std::max(tile_elems, rows * c->n[0]);
+    walls |= c->plan.walls;
+  }
+  std::vector<Tile> tiles;
+  for (size_t m = 0; m < b->members.size(); m++) {
+    hlbm_ctx* c = b->members[m];
+    for (int z = 0; z < c->n[2]; z++)
+      for (int y0 = 0; y0 < c->n[1]; y0 += rows_of[m])
+        tiles.push_back(make_int4(int(m), z, y0, std::min(rows_of[m], c->n[1] - y0)));
+  }
+  const size_t stage_bytes = size_t(Q) * tile_elems * es;
+  const size_t head = tma_head_bytes();
+  int stages = stage_bytes ? int((226 * 1024 - head) / stage_bytes) : 0;
+  int stages2 = stage_bytes ? int((112 * 1024 - head) / stage_bytes) : 0;
+  stages = stages > 4 ? 4 : stages;
+  stages2 = stages2 > 4 ? 4 : stages2;
+  if (b->variant < 8 && !b->members.empty() && stages < 2)
+    return batch_fail(HLBM_EPLAN, "batch tiles do not fit two pipeline stages");
+  b->stages2 = stages2;
+  if (b->members.size() > b->desc_cap) {
+    cudaFree(b->desc_dev);
+    b->desc_cap = std::max<size_t>(b->members.size(), 2 * b->desc_cap);
+    if (cudaMalloc(&b->desc_dev, b->desc_cap * sizeof(LatticeDesc)) != cudaSuccess)
+      return batch_fail(HLBM_ENOMEM, "batch descriptors");
+  }
+  if (tiles.size() > b->tiles_cap) {
+    cudaFree(b->tiles_dev);
+    b->tiles_cap = std::max<size_t>(tiles.size(), 2 * b->tiles_cap);
+    if (cudaMalloc(&b->tiles_dev, b->tiles_cap * sizeof(Tile)) != cudaSuccess)
+      return batch_fail(HLBM_ENOMEM, "batch tile list");
+  }
+  if (!tiles.empty())
+    HLBM_CK(cudaMemcpyAsync(b->tiles_dev, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                            b->stream));
+  HLBM_CK(cudaStreamSynchronize(b->stream));
+  b->ntiles = int(tiles.size());
+  b->tile_elems = tile_elems;
+  b->stages = stages;
+  b->walls = walls;
+  b->dirty = false;
+  b->descs_stale = true;
+  return HLBM_OK;
+}
+
+// upload the members' descriptors: buffers, current index, first-step flag
+int batch_refresh_descs(hlbm_batch* b) {
+  if (!b->descs_stale) return HLBM_OK;
+  std::vector<LatticeDesc> descs(b->members.size());
+  for (size_t m = 0; m < b->members.size(); m++) {
+    hlbm_ctx* c = b->members[m];
+    descs[m].plan = c->plan_dev;
+    descs[m].f[0] = c->f[0];
+    descs[m].f[1] = c->f[1];
+    descs[m].flags = c->flags;
+    descs[m].cur = c->cur;
+    descs[m].prologue = c->phase == RAW ? 1 : 0;
+  }
+  if (!descs.empty())
+    HLBM_CK(cudaMemcpyAsync(b->desc_dev, descs.data(), descs.size() * sizeof(LatticeDesc), cudaMemcpyHostToDevice,
+                            b->stream));
+  HLBM_CK(cudaStreamSynchronize(b->stream));
+  b->descs_stale = false;
+  return HLBM_OK;
+}
+
+cudaError_t batch_launch(hlbm_batch* b, int parity) {
+  TmaArgs t;
+  t.desc = b->desc_dev;
+  t.tiles = b->tiles_dev;
+  t.ntiles = b->ntiles;
+  t.tile_elems = b->tile_elems;
+  t.ctas_per_sm = (b->variant == 6 && b->stages2 >= 2) ? 2 : 1;
+  t.stages = t.ctas_per_sm == 2 ? b->stages2 : b->stages;
+  t.parity = parity;
+  t.err = b->err_dev;
+  t.grid = std::min(b->ntiles, b->sms * t.ctas_per_sm);
+  StepPlan dummy;
+  std::memset(&dummy, 0, sizeof(dummy));
+  b->launches++;
+  switch (b->precision) {
+    case HLBM_F64: return step_f64(MODE_FUSED, b->walls, nullptr, nullptr, nullptr, dummy, b->stream, b->variant, t);
+    case HLBM_F64_STRICT: return step_f64_strict(MODE_FUSED, b->walls, nullptr, nullptr, nullptr, dummy, b->stream, b->variant, t);
+    case HLBM_F32: return step_f32(MODE_FUSED, b->walls, nullptr, nullptr, nullptr, dummy, b->stream, b->variant, t);
+    case HLBM_F16: return step_f16(MODE_FUSED, b->walls, nullptr, nullptr, nullptr, dummy, b->stream, b->variant, t);
+    default: return step_bf16(MODE_FUSED, b->walls, nullptr, nullptr, nullptr, dummy, b->stream, b->variant, t);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hlbm_batch_create(int32_t precision, int32_t device, hlbm_batch** out) {
+  if (!out || precision < HLBM_F64 || precision > HLBM_BF16) return fail(HLBM_EINVAL, "hlbm_batch_create: bad argument");
+  *out = nullptr;
+  auto* b = new hlbm_batch();
+  b->precision = precision;
+  b->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->err_dev, sizeof(int)) != cudaSuccess || cudaMemset(b->err_dev, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    hlbm_batch_destroy(b);
+    return fail(HLBM_ECUDA, "hlbm_batch_create: cannot set up the device");
+  }
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+  *out = b;
+  return HLBM_OK;
+}
+
+int hlbm_batch_add(hlbm_batch* b, hlbm_ctx* c) {
+  if (!b || !c) return fail(HLBM_EINVAL, "hlbm_batch_add: NULL argument");
+  if (c->precision != b->precision || c->device != b->device)
+    return fail(HLBM_EINVAL, "hlbm_batch_add: lattice precision or device differs from the batch");
+  for (hlbm_ctx* m : b->members)
+    if (m == c) return fail(HLBM_EINVAL, "hlbm_batch_add: lattice already in the batch");
+  if (b->variant < 8 && (size_t(c->n[0]) * elem_size(c->precision)) % 16 != 0)
+    return fail(HLBM_EPLAN, "hlbm_batch_add: the pipelined batch kernel needs nx * bytes per population % 16 == 0");
+  b->members.push_back(c);
+  b->dirty = true;
+  return HLBM_OK;
+}
+
+int hlbm_batch_remove(hlbm_batch* b, hlbm_ctx* c) {
+  if (!b || !c) return fail(HLBM_EINVAL, "hlbm_batch_remove: NULL argument");
+  for (size_t m = 0; m < b->members.size(); m++)
+    if (b->members[m] == c) {
+      b->members.erase(b->members.begin() + m);
+      b->dirty = true;
+      return HLBM_OK;
+    }
+  return fail(HLBM_EINVAL, "hlbm_batch_remove: lattice not in the batch");
+}
+
+int hlbm_batch_step(hlbm_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 0) return fail(HLBM_EINVAL, "hlbm_batch_step: bad argument");
+  if (nsteps == 0 || b->members.empty()) return HLBM_OK;
+  HLBM_CK(cudaSetDevice(b->device));
+  b->descs_stale = true;  // members may have been read out or rewritten since the last call
+  bool fresh = false;
+  for (hlbm_ctx* c : b->members) {
+    if (int rc = build_plan(c)) return rc;
+    if (c->phase == MATER) c->phase = POSTCOL;
+    fresh |= c->phase == RAW;
+    HLBM_CK(cudaStreamSynchronize(c->stream));  // member work is ordered before the batch stream's
+  }
+  if (int rc = batch_rebuild(b)) return rc;
+  if (int rc = batch_refresh_descs(b)) return rc;
+  int64_t todo = nsteps;
+  int parity = 0;
+  if (fresh) {  // fresh members take their first step (collide S_0) inside this launch
+    HLBM_CK(batch_launch(b, 0));
+    for (hlbm_ctx* c : b->members) {
+      c->steps++;
+      c->cur = 1 - c->cur;
+      c->phase = POSTCOL;
+    }
+    b->descs_stale = true;
+    if (int rc = batch_refresh_descs(b)) return rc;
+    todo--;
+  }
+  if (!b->graph && todo >= 2) {
+    cudaGraph_t g;
+    HLBM_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e0 = batch_launch(b, 0);
+    cudaError_t e1 = batch_launch(b, 1);
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    b->launches -= 2;
+    if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess)
+      return fail(HLBM_ECUDA, "hlbm_batch_step: graph capture failed");
+    cudaError_t e3 = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return fail(HLBM_ECUDA, "hlbm_batch_step: graph instantiation failed");
+  }
+  while (todo >= 2) {
+    HLBM_CK(cudaGraphLaunch(b->graph, b->stream));
+    b->replays++;
+    b->launches += 2;
+    todo -= 2;
+  }
+  if (todo == 1) {
+    HLBM_CK(batch_launch(b, 0));
+    parity = 1;
+  }
+  // the graph replays leave cur unchanged; a trailing single launch flips it
+  for (hlbm_ctx* c : b->members) {
+    c->steps += nsteps - (fresh ? 1 : 0);
+    if (parity) c->cur = 1 - c->cur;
+  }
+  if (parity) b->descs_stale = true;
+  HLBM_CK(cudaStreamSynchronize(b->stream));
+  int e = 0;
+  HLBM_CK(cudaMemcpy(&e, b->err_dev, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(b->err_dev, 0, sizeof(int));
+    return fail(HLBM_ECUDA, "hlbm_batch_step: a shared-memory pipeline wait timed out");
+  }
+  return HLBM_OK;
+}
+
+int hlbm_batch_tune(hlbm_batch* b, int32_t variant) {
+  if (!b || variant < 6 || variant > 9) return fail(HLBM_EINVAL, "hlbm_batch_tune: variant must be 6, 7, 8 or 9");
+  if (variant < 8)
+    for (hlbm_ctx* c : b->members)
+      if ((size_t(c->n[0]) * elem_size(c->precision)) % 16 != 0)
+        return fail(HLBM_EPLAN, "hlbm_batch_tune: a member's rows do not suit the pipelined kernel");
+  b->variant = variant;
+  b->dirty = true;
+  return HLBM_OK;
+}
+
+int hlbm_batch_info(hlbm_batch* b, int64_t info[6]) {
+  if (!b || !info) return fail(HLBM_EINVAL, "hlbm_batch_info: NULL argument");
+  if (int rc = batch_rebuild(b)) return rc;
+  info[0] = int64_t(b->members.size());
+  info[1] = b->ntiles;
+  info[2] = b->tile_elems;
+  info[3] = b->stages;
+  info[4] = b->replays;
+  info[5] = b->launches;
+  return HLBM_OK;
+}
+
+int hlbm_batch_destroy(hlbm_batch* b) {
+  if (!b) return HLBM_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  cudaFree(b->desc_dev);
+  cudaFree(b->tiles_dev);
+  cudaFree(b->err_dev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return HLBM_OK;
+}
 
 }  // extern "C"

@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "lbm_step_tiles.cuh"
+#include "lbm_step_tma.cuh"
 #include "lbm_step_vec.cuh"
 
 namespace hlbm {
@@ -22,8 +24,14 @@ template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int MINB>
 cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
   dim3 grid, block;
   step_geometry(p, grid, block);
-  k_step<S, R, STRICT, MODE, WALLS, true, MINB>
-      <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
+  const S* fi = static_cast<const S*>(fin);
+  S* fo = static_cast<S*>(fout);
+  if (MODE == MODE_FUSED && p.collision == 0)
+    k_step<S, R, STRICT, MODE, WALLS, 0, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+  else if (MODE == MODE_FUSED)
+    k_step<S, R, STRICT, MODE, WALLS, 1, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+  else
+    k_step<S, R, STRICT, MODE, WALLS, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   return cudaGetLastError();
 }
 
@@ -55,15 +63,63 @@ cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const S
   constexpr int NPT = vec_npt<S>();
   dim3 grid, block;
   vec_geometry(p, NPT, 0, grid, block);
-  k_step_vec<S, R, STRICT, MODE, NPT, MINB>
-      <<<grid, block, 0, s>>>(static_cast<const S*>(fin), static_cast<S*>(fout), flags, p);
+  const S* fi = static_cast<const S*>(fin);
+  S* fo = static_cast<S*>(fout);
+  if (MODE == MODE_FUSED && p.collision == 0)
+    k_step_vec<S, R, STRICT, MODE, NPT, 0, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+  else if (MODE == MODE_FUSED)
+    k_step_vec<S, R, STRICT, MODE, NPT, 1, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+  else
+    k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   return cudaGetLastError();
 }
 
-// Step kernel variants: variant % 2 selects the kernel (0: one node per thread, 1: vectorised
-// when eligible), variant / 2 the occupancy target: at least 1, 2 or 3 blocks of 256 threads per
-// SM (__launch_bounds__ minimum blocks, which caps registers at 255, 128 or 85 per thread).
-constexpr int NUM_VARIANTS = 6;
+// Step kernel variants 0..5: variant % 2 selects the kernel (0: one node per thread, 1:
+// vectorised when eligible), variant / 2 the occupancy target: at least 1, 2 or 3 blocks of 256
+// threads per SM (__launch_bounds__ minimum blocks, which caps registers at 255, 128 or 85 per
+// thread).  Variants 6 and 7: the bulk-copy pipelined persistent kernel (lbm_step_tma.cuh), with
+// tiles of about 512 (variant 6) or 1024 (variant 7) nodes; fused steps only, when eligible.
+constexpr int NUM_VARIANTS = 8;
+
+// what the pipelined kernel needs besides the plan
+struct TmaArgs {
+  const LatticeDesc* desc = nullptr;
+  const Tile* tiles = nullptr;
+  int ntiles = 0;
+  int tile_elems = 0;  // elements of one direction in a stage
+  int stages = 0;      // 0: not eligible
+  int parity = 0;
+  int* err = nullptr;
+  int grid = 0;
+  int ctas_per_sm = 1;
+};
+
+template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
+cudaError_t launch_tma_t(const TmaArgs& a, cudaStream_t s) {
+  auto kern = k_step_tma<S, R, STRICT, STAGES, WALLS, MINB>;
+  const size_t smem = tma_smem_bytes(STAGES, a.tile_elems, sizeof(S));
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<a.grid, TMA_THREADS, smem, s>>>(a.desc, a.tiles, a.ntiles, a.tile_elems, a.parity, a.err);
+  return cudaGetLastError();
+}
+
+template <typename S, typename R, bool STRICT, bool WALLS, int MINB>
+cudaError_t launch_tma_stages(const TmaArgs& a, cudaStream_t s) {
+  switch (a.stages) {
+    case 2: return launch_tma_t<S, R, STRICT, 2, WALLS, MINB>(a, s);
+    case 3: return launch_tma_t<S, R, STRICT, 3, WALLS, MINB>(a, s);
+    default: return launch_tma_t<S, R, STRICT, 4, WALLS, MINB>(a, s);
+  }
+}
+
+// ctas_per_sm: 1 or 2 (the stages of two CTAs must fit one SM's shared memory)
+template <typename S, typename R, bool STRICT>
+cudaError_t launch_tma(const TmaArgs& a, int walls, int ctas_per_sm, cudaStream_t s) {
+  if (ctas_per_sm == 2)
+    return walls ? launch_tma_stages<S, R, STRICT, true, 2>(a, s) : launch_tma_stages<S, R, STRICT, false, 2>(a, s);
+  return walls ? launch_tma_stages<S, R, STRICT, true, 1>(a, s) : launch_tma_stages<S, R, STRICT, false, 1>(a, s);
+}
 
 template <typename S, typename R, bool STRICT, int MINB>
 cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fout, const int8_t* flags,
@@ -83,9 +139,27 @@ cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fo
                : launch_one<S, R, STRICT, MODE_FINISH, false, MINB>(fin, fout, flags, p, s);
 }
 
+// tile-list kernel of batches (variant 8: >= 3 CTAs per SM, 9: >= 2)
+template <typename S, typename R, bool STRICT>
+cudaError_t launch_tiles(const TmaArgs& a, int walls, int variant, cudaStream_t s) {
+  if (variant == 9) {
+    if (walls) k_step_tiles<S, R, STRICT, true, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+    else k_step_tiles<S, R, STRICT, false, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+  } else {
+    if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+    else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+  }
+  return cudaGetLastError();
+}
+
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                        cudaStream_t s, int variant) {
+                        cudaStream_t s, int variant, const TmaArgs& tma) {
+  if (variant >= 8) return launch_tiles<S, R, STRICT>(tma, walls, variant, s);
+  if (variant >= 6) {
+    if (mode == MODE_FUSED && tma.stages >= 2) return launch_tma<S, R, STRICT>(tma, walls, tma.ctas_per_sm, s);
+    variant = 4;
+  }
   const bool vec = (variant % 2) == 1 && vec_eligible<S>(p, walls);
   switch (variant / 2) {
     case 0: return launch_minb<S, R, STRICT, 1>(mode, walls, vec, fin, fout, flags, p, s);
@@ -96,14 +170,14 @@ cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const 
 
 // one entry per precision tier (defined in step_*.cu)
 cudaError_t step_f64_strict(int mode, int walls, const void* fin, void* fout, const int8_t* flags,
-                            const StepPlan& p, cudaStream_t s, int variant);
+                            const StepPlan& p, cudaStream_t s, int variant, const TmaArgs& tma);
 cudaError_t step_f64(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s, int variant);
+                     cudaStream_t s, int variant, const TmaArgs& tma);
 cudaError_t step_f32(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s, int variant);
+                     cudaStream_t s, int variant, const TmaArgs& tma);
 cudaError_t step_f16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                     cudaStream_t s, int variant);
+                     cudaStream_t s, int variant, const TmaArgs& tma);
 cudaError_t step_bf16(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
-                      cudaStream_t s, int variant);
+                      cudaStream_t s, int variant, const TmaArgs& tma);
 
 }  // namespace hlbm

@@ -443,14 +443,21 @@ __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, 
   }
 }
 
-// ------------------------------------------------------------------ the step kernel
-template <typename S, typename R, bool STRICT, int MODE, bool WALLS, bool PLANES, int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout,
-                                              const int8_t* __restrict__ flags, const StepPlan p) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= p.nx || y >= p.ny) return;
+// ------------------------------------------------------------------ one node of the step
+// COLL: 0 BGK, 1 MRT, 2 chosen at run time by p.collision (mixed batches, read-out modes).
+template <typename R, bool STRICT, int COLL>
+__device__ __forceinline__ void collide(R (&v)[Q], const StepPlan& p) {
+  if (COLL == 0 || (COLL == 2 && p.collision == 0))
+    bgk<R, STRICT>(v, p);
+  else
+    mrt<R, STRICT>(v, p);
+}
+
+// The whole step for the node (x, y, z): gather (pull with periodic wrap and on-node
+// bounce-back), boundary operators, start_iteration boxes, collision, store.
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL>
+__device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restrict__ fout,
+                                          const int8_t* __restrict__ flags, const StepPlan& p, int x, int y, int z) {
   const int64_t idx = ((int64_t)z * p.ny + y) * p.nx + x;
   const int8_t flag = flags[idx];
   if (WALLS && flag == FLAG_WALL) {
@@ -493,10 +500,8 @@ __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S
       const S raw = ld_stream(ptr);
       v[I] = bounce ? Codec<S, R>::template dec<O>(raw, p) : Codec<S, R>::template dec<I>(raw, p);
     });
-    if (PLANES) {
-      const bool boundary = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
-      if (boundary) plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
-    }
+    const bool boundary = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
+    if (boundary && p.nops > 0) plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
   }
   if (MODE != MODE_FINISH) {
     for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
@@ -504,14 +509,20 @@ __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S
       if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
         Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
     }
-    if (flag == FLAG_FLUID) {
-      if (p.collision == 0)
-        bgk<R, STRICT>(v, p);
-      else
-        mrt<R, STRICT>(v, p);
-    }
+    if (flag == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
   }
   Unroll<0, Q>::run([&]<int I>() { fout[I * p.stride + idx] = Codec<S, R>::template enc<I>(v[I], p); });
+}
+
+// ------------------------------------------------------------------ the step kernel
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout,
+                                                    const int8_t* __restrict__ flags, const StepPlan p) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= p.nx || y >= p.ny) return;
+  node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
 }
 
 }  // namespace hlbm

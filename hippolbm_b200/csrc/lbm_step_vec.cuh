@@ -181,7 +181,7 @@ __device__ __forceinline__ void load_flags(const int8_t* p, int8_t (&fl)[NPT]) {
 }
 
 // ------------------------------------------------------------------ the kernel
-template <typename S, typename R, bool STRICT, int MODE, int NPT, int MINB = 1>
+template <typename S, typename R, bool STRICT, int MODE, int NPT, int COLL, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fin, S* __restrict__ fout,
                                                      const int8_t* __restrict__ flags, const StepPlan p) {
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;  // vector index along x
@@ -274,12 +274,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
         if (x >= b.lo[0] && x <= b.hi[0] && yy >= b.lo[1] && yy <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
           Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
       }
-      if (fl[K] == FLAG_FLUID) {
-        if (p.collision == 0)
-          bgk<R, STRICT>(v, p);
-        else
-          mrt<R, STRICT>(v, p);
-      }
+      if (fl[K] == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
     }
     Unroll<0, Q>::run([&]<int I>() { c[I].template set<K>(Codec<S, R>::template enc<I>(v[I], p)); });
   });

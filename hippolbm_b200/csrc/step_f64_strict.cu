@@ -3,7 +3,7 @@
 #include "launch.cuh"
 namespace hlbm {
 cudaError_t step_f64_strict(int mode, int walls, const void* fin, void* fout, const int8_t* flags,
-                            const StepPlan& p, cudaStream_t s, int variant) {
-  return launch_step<double, double, true>(mode, walls, fin, fout, flags, p, s, variant);
+                            const StepPlan& p, cudaStream_t s, int variant, const TmaArgs& tma) {
+  return launch_step<double, double, true>(mode, walls, fin, fout, flags, p, s, variant, tma);
 }
 }  // namespace hlbm

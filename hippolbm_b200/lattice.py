@@ -147,6 +147,21 @@ class Lattice:
         capi.check(self.L.hlbm_simulation_state(self.h, out))
         return tuple(out)
 
+    def residual(self) -> float:
+        out = C.c_double()
+        capi.check(self.L.hlbm_residual(self.h, C.byref(out)))
+        return out.value
+
+    def moments(self) -> tuple:
+        out = (C.c_double * 4)()
+        capi.check(self.L.hlbm_moments(self.h, out))
+        return tuple(out)
+
+    def wall_force(self) -> tuple:
+        out = (C.c_double * 3)()
+        capi.check(self.L.hlbm_wall_force(self.h, out))
+        return tuple(out)
+
     def parameters(self) -> dict:
         out = (C.c_double * 9)()
         capi.check(self.L.hlbm_get_parameters(self.h, out))
@@ -168,9 +183,9 @@ class Lattice:
         """Time every step-kernel variant on this lattice (state unchanged) and keep the fastest;
         returns (chosen variant, {variant: ms per step})."""
         chosen = C.c_int32(0)
-        ms = (C.c_double * 6)()
+        ms = (C.c_double * 8)()
         capi.check(self.L.hlbm_autotune(self.h, int(reps), C.byref(chosen), ms))
-        return chosen.value, {v: ms[v] for v in range(6) if ms[v] >= 0}
+        return chosen.value, {v: ms[v] for v in range(8) if ms[v] >= 0}
 
     def stream_handle(self) -> int:
         return self.L.hlbm_stream(self.h) or 0

@@ -136,6 +136,16 @@ int hlbm_macro_variables(hlbm_ctx* ctx, double* rho, double* u);
  * nodes, FP64 on the device. */
 int hlbm_simulation_state(hlbm_ctx* ctx, double out[3]);
 
+/* FP64 reductions on the device (no reference counterparts; used by the precision study and the
+ * solve server).  hlbm_residual: relative L2 change of the velocity field since the previous call
+ * on this context, sqrt(sum |u - u_prev|^2 / sum |u|^2) (HUGE_VAL on the first call; keeps an
+ * FP32 velocity snapshot on the device).  hlbm_moments: {sum rho, sum rho u_x, sum rho u_y,
+ * sum rho u_z} over fluid nodes.  hlbm_wall_force: force on the wall obstacles by momentum exchange,
+ * sum over fluid-to-wall links of 2 f*_i e_i, from the post-collision state (after >= 1 step). */
+int hlbm_residual(hlbm_ctx* ctx, double* out);
+int hlbm_moments(hlbm_ctx* ctx, double out[4]);
+int hlbm_wall_force(hlbm_ctx* ctx, double out[3]);
+
 /* populations of the current state (FP64, layout above); put replaces them */
 int hlbm_get_populations(hlbm_ctx* ctx, double* out);
 int hlbm_put_populations(hlbm_ctx* ctx, const double* in);
@@ -145,18 +155,42 @@ int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
 
 /* info = {nx, ny, nz, precision, steps done, kernel launches, bytes per population, device} */
 int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
-/* Step kernel selection (no reference counterpart).  variant % 2 picks the kernel: 0 = one node
- * per thread, 1 = vectorised (consecutive x-nodes per thread in one vector per direction plane;
- * used when the lattice has no wall obstacles and nx splits into >= 32 vectors, else the first
- * kernel runs); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256 threads per SM.
- * hlbm_autotune times `reps` fused launches of every variant on this lattice (from the current
- * populations into the idle buffer, so the state does not advance), keeps the fastest, and
- * returns it in *chosen and the per-variant times (ms, -1 if skipped) in ms_per_variant[6]. */
-#define HLBM_NUM_VARIANTS 6
+/* Step kernel selection (no reference counterpart).  Variants 0..5: variant % 2 picks the kernel,
+ * 0 = one node per thread, 1 = vectorised (consecutive x-nodes per thread in one vector per
+ * direction plane; used when the lattice has no wall obstacles and nx splits into >= 32 vectors,
+ * else the first kernel runs); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256
+ * threads per SM.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
+ * into shared-memory stages (256 or 512 threads per CTA; needs nx * bytes per population to be a
+ * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
+ * variant on this lattice (from the current populations into the idle buffer, so the state does
+ * not advance), keeps the fastest, and returns it in *chosen and the per-variant times (ms, -1 if
+ * skipped) in ms_per_variant[HLBM_NUM_VARIANTS]. */
+#define HLBM_NUM_VARIANTS 8
 int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------------------
+ * Batches (no reference counterpart).  A batch advances many independent lattices -- contexts
+ * made with hlbm_domain on the same device and precision, each with its own size, plan, collision
+ * and boundary operators -- with ONE launch of the pipelined persistent kernel per time step, over
+ * the concatenated tile list of all members; steps are replayed from a captured CUDA graph of two
+ * steps.  Kernel (hlbm_batch_tune): 8 (default) / 9 = one CTA per tile of about 256 nodes with
+ * direct pulls (at least 3 / 2 CTAs per SM), any lattice shape; 6 / 7 = the pipelined kernel
+ * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0).  A
+ * member that has not stepped yet takes its first step inside the batched launch.  While a
+ * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.
+ * hlbm_batch_step(b, n) advances every member n steps. */
+typedef struct hlbm_batch hlbm_batch;
+int hlbm_batch_create(int32_t precision, int32_t device, hlbm_batch** out);
+int hlbm_batch_add(hlbm_batch* b, hlbm_ctx* lattice);
+int hlbm_batch_remove(hlbm_batch* b, hlbm_ctx* lattice);
+int hlbm_batch_step(hlbm_batch* b, int64_t nsteps);
+int hlbm_batch_tune(hlbm_batch* b, int32_t variant);
+/* info = {members, tiles, tile elements, stages, graph replays, kernel launches} */
+int hlbm_batch_info(hlbm_batch* b, int64_t info[6]);
+int hlbm_batch_destroy(hlbm_batch* b);
 
 /* simulation_state for callers that cannot allocate device memory, such as an analysis hook
  * inside a host application that owns the whole device budget, or a loop that must not pay
