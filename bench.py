@@ -8,6 +8,14 @@ operator does (log.cpp:74-88).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision f64|f64_strict|f32|f16|bf16] [--collision bgk|mrt] [--n 512]
+    python bench.py --workload precision|batch|serve [...]
+
+Other workloads, one JSON line each: `precision` (MRT flow past a sphere in a 1024x256x256
+channel, 20000 steps, at FP64 / FP32 / FP16 / BF16 storage: velocity L2 error, mass drift and drag
+against the FP64 run), `batch` (256 independent lattices of mixed sizes and decks in FP32, one
+launch per step for all of them, against the same lattices stepped one at a time) and `serve`
+(Poisson request streams served by continuous batching with FP16 storage against the plain FP64
+path serving the same stream, one request at a time).
 
 The default arm prints one JSON line with the device-timed throughput (`value`), the end-to-end
 figure through the C-ABI with host buffers (`e2e`), the fused kernel's roofline against the
@@ -52,6 +60,20 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=128, help="lattice edge of the CPU baseline sample")
     ap.add_argument("--variant", type=int, default=-1, help="step-kernel variant; -1: autotune")
+    ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
+                    help="16-bit storage rounding")
+    ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="precision workload: linear scale of the 1024x256x256 channel (steps scale alike)")
+    ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,f16:shift,bf16",
+                    help="precision workload: storage tiers; options after ':' joined by '+': "
+                         "nearest (round-to-nearest storage), shift (deviations from feq at the inflow)")
+    ap.add_argument("--members", type=int, default=256, help="batch workload: lattices")
+    ap.add_argument("--member-steps", type=int, default=2000, help="batch workload: steps of every lattice")
+    ap.add_argument("--alone-steps", type=int, default=200,
+                    help="batch workload: steps per lattice of the one-at-a-time comparison")
+    ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per stream")
+    ap.add_argument("--rates", default="10,100,1000", help="serve workload: arrival rates (req/s)")
     return ap.parse_args()
 
 
@@ -207,6 +229,7 @@ def run_ours(a):
     device = torch.device("cuda", local)
     case = make_case(a)
     lat = Lattice.from_case(case, a.precision, device=local)
+    lat.rounding(a.rounding)
     stream = torch.cuda.ExternalStream(lat.stream_handle(), device=device)
     nodes = lat.ncell
     # the project's autotuner picks the step-kernel variant on this lattice (state unchanged)
@@ -244,6 +267,7 @@ def run_ours(a):
     # pinned memory, one solve of e2e_steps time steps, D2H of simulation_state.
     e2e = None
     lat = Lattice.from_case(case, a.precision, device=local)
+    lat.rounding(a.rounding)
     lat.tune(variant)
     init = torch.empty(19 * nodes, dtype=torch.float64, pin_memory=True)
     w = [1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12  # rest equilibrium, rho = 1
@@ -295,7 +319,7 @@ def run_ours(a):
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision],
                "data": "synthetic",
                "config": {"workload": workload_name(a), "nodes": [a.n] * 3, "collision": a.collision,
-                          "tau": a.tau, "u_wall": 0.05, "precision": a.precision,
+                          "tau": a.tau, "u_wall": 0.05, "precision": a.precision, "rounding": a.rounding,
                           "l2": f"inputs larger than L2: {2 * 19 * nodes * bpp / 1e9:.1f} GB of populations",
                           "parallelism": f"replicas x{world}", "state_after": list(state),
                           "kernel_variant": variant,
@@ -310,10 +334,121 @@ def run_ours(a):
     return 0
 
 
+# ------------------------------------------------------------------ other workloads
+def run_precision(a):
+    from hippolbm_b200.deck import sphere_channel_case
+    from hippolbm_b200.precision import precision_study
+
+    k = a.scale
+    nodes = (int(round(1024 * k)), int(round(256 * k)), int(round(256 * k)))
+    steps = int(round(20000 * k))
+    case = sphere_channel_case(nodes, (256 * k, 128 * k, 128 * k), 24 * k, tau=0.56, u_in=0.04, steps=steps)
+    t0 = time.perf_counter()
+    recs = precision_study(case, tuple(a.tiers.split(",")), steps)
+    by = {r["precision"]: r for r in recs}
+    low = by.get("f16") or recs[-1]
+    line = {"workload": "precision", "metric": "rel_l2_velocity_error", "value": low["l2_u"], "unit": "1",
+            "tier": low["precision"], "higher_is_better": False, "n_gpus": 1, "steps": steps,
+            "data": "synthetic", "dtype": "f64 / f32 / f32 (f16 storage) / f32 (bf16 storage)",
+            "config": {"workload": f"sphere_channel_{nodes[0]}x{nodes[1]}x{nodes[2]}_mrt_tau0.56_u0.04",
+                       "sphere": {"center": [256 * k, 128 * k, 128 * k], "radius": 24 * k},
+                       "mrt_rates": list(case.mrt_rates), "outlet": "zero_gradient", "inlet": "neumann u_x=0.04"},
+            "tiers": recs, "wall_s": round(time.perf_counter() - t0, 1)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(a):
+    import torch
+
+    from hippolbm_b200.batch import Batch
+    from hippolbm_b200.deck import mixed_batch_cases
+    from hippolbm_b200.lattice import Lattice
+
+    torch.cuda.set_device(0)
+    cases = mixed_batch_cases(a.members, steps=a.member_steps)
+    lats = [Lattice.from_case(c, "f32") for c in cases]
+    nodes = sum(l.ncell for l in lats)
+    batch = Batch("f32")
+    for l in lats:
+        batch.add(l)
+    stream = torch.cuda.ExternalStream(batch.stream_handle(), device=torch.device("cuda", 0))
+    batch.step(a.warmup)
+    torch.cuda.synchronize()
+    info0 = batch.info()
+    clocks = ClockSampler(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(a.member_steps - a.warmup)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    timed = a.member_steps - a.warmup
+    info = batch.info()
+    mlups = nodes * timed / (ms * 1e-3) / 1e6
+    batch.close()
+    for l in lats:
+        l.close()
+    # the same lattices one at a time, each with its own launches (variant 0, no graph)
+    alone_ms = 0.0
+    for c in cases:
+        with Lattice.from_case(c, "f32") as l:
+            l.step(3)
+            s = torch.cuda.ExternalStream(l.stream_handle(), device=torch.device("cuda", 0))
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(s)
+            l.step(a.alone_steps)
+            f1.record(s)
+            f1.synchronize()
+            alone_ms += f0.elapsed_time(f1)
+    alone = nodes * a.alone_steps / (alone_ms * 1e-3) / 1e6
+    kinds = {}
+    for c in cases:
+        kinds[c.name.split("_")[1]] = kinds.get(c.name.split("_")[1], 0) + 1
+    line = {"workload": "batch", "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": 1,
+            "steps": timed, "warmup": a.warmup, "ms_per_step": round(ms / timed, 4), "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"mixed_batch_{a.members}", "members": a.members, "nodes": nodes,
+                       "kinds": kinds, "seed": 20261203, "kernel_variant": 8},
+            "one_at_a_time_mlups": round(alone, 1), "speedup_vs_one_at_a_time": round(mlups / alone, 2),
+            "gpu_launches": info["launches"] - info0["launches"], "graph_replays": info["graph_replays"] - info0["graph_replays"],
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(a):
+    from hippolbm_b200 import serve
+
+    lines = []
+    for rate in [float(r) for r in a.rates.split(",")]:
+        fast = serve.serve_batched(serve.make_stream(rate, a.requests), "f16", hbm_budget=160e9)
+        plain = serve.serve_plain(serve.make_stream(rate, a.requests), "f64")
+        lines.append({"rate": rate, "batched_f16": fast, "plain_f64": plain,
+                      "mlups_ratio": round(fast["aggregate_mlups"] / plain["aggregate_mlups"], 2)})
+    top = lines[-1]
+    line = {"workload": "serve", "metric": "aggregate MLUPS", "value": top["batched_f16"]["aggregate_mlups"],
+            "unit": "MLUPS", "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (f16 storage)",
+            "data": "synthetic",
+            "config": {"workload": f"poisson_stream_{a.requests}_requests", "requests": a.requests,
+                       "rates": a.rates, "hbm_budget_gb": 160, "edges": [24, 192], "budgets": [500, 20000],
+                       "residual_tol": 1e-6},
+            "sweep": lines}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "precision":
+        return run_precision(a)
+    if a.workload == "batch":
+        return run_batch(a)
+    if a.workload == "serve":
+        return run_serve(a)
     return run_ours(a)
 
 

@@ -39,6 +39,9 @@ class Batch:
         capi.check(self.L.hlbm_batch_info(self.h, out))
         return dict(zip(["members", "tiles", "tile_elems", "stages", "graph_replays", "launches"], list(out)))
 
+    def stream_handle(self) -> int:
+        return self.L.hlbm_batch_stream(self.h) or 0
+
     def close(self):
         if self.h and self.h.value:
             self.L.hlbm_batch_destroy(self.h)

@@ -32,7 +32,10 @@ SIGNATURES = {
     "hlbm_get_parameters": (C.c_int, [_vp, _d3]),
     "hlbm_collision": (C.c_int, [_vp, C.c_int32, _d3]),
     "hlbm_storage_scale": (C.c_int, [_vp, C.c_double, C.c_double]),
+    "hlbm_storage_rounding": (C.c_int, [_vp, C.c_int32]),
+    "hlbm_storage_reference": (C.c_int, [_vp, C.c_double, _d3]),
     "hlbm_set_distribution": (C.c_int, [_vp, C.c_double, _d3, C.c_int32]),
+    "hlbm_init_double_couette": (C.c_int, [_vp, _d3, C.c_int32]),
     "hlbm_init_obstacles": (C.c_int, [_vp]),
     "hlbm_register_solid_ball": (C.c_int, [_vp, C.c_int32, _d3, C.c_double]),
     "hlbm_register_solid_wall": (C.c_int, [_vp, C.c_int32, _d3, _d3]),
@@ -46,15 +49,20 @@ SIGNATURES = {
     "hlbm_neumann": (C.c_int, [_vp, C.c_int32, _d3, _i3, C.c_int32]),
     "hlbm_lid_driven_cavity": (C.c_int, [_vp, C.c_int32, _d3, _i3, C.c_int32]),
     "hlbm_start_set_distribution": (C.c_int, [_vp, C.c_double, _d3]),
+    "hlbm_zero_gradient": (C.c_int, [_vp, C.c_int32, _i3, C.c_int32]),
     "hlbm_step": (C.c_int, [_vp, C.c_int64]),
     "hlbm_sync": (C.c_int, [_vp]),
     "hlbm_macro_variables": (C.c_int, [_vp, _d3, _d3]),
     "hlbm_simulation_state": (C.c_int, [_vp, _d3]),
+    "hlbm_plane_velocity_profile": (C.c_int, [_vp, C.c_int32, _d3, _d3, _d3, C.POINTER(C.c_int64)]),
     "hlbm_residual": (C.c_int, [_vp, _d3]),
     "hlbm_moments": (C.c_int, [_vp, _d3]),
     "hlbm_wall_force": (C.c_int, [_vp, _d3]),
     "hlbm_get_populations": (C.c_int, [_vp, _d3]),
     "hlbm_put_populations": (C.c_int, [_vp, _d3]),
+    "hlbm_checkpoint_bytes": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "hlbm_checkpoint_save": (C.c_int, [_vp, _vp, C.c_int64]),
+    "hlbm_checkpoint_load": (C.c_int, [_vp, _vp, C.c_int64]),
     "hlbm_get_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
     "hlbm_put_flags": (C.c_int, [_vp, C.POINTER(C.c_int8)]),
     "hlbm_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
@@ -67,6 +75,7 @@ SIGNATURES = {
     "hlbm_batch_step": (C.c_int, [_vp, C.c_int64]),
     "hlbm_batch_tune": (C.c_int, [_vp, C.c_int32]),
     "hlbm_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "hlbm_batch_stream": (_vp, [_vp]),
     "hlbm_batch_destroy": (C.c_int, [_vp]),
     "hlbm_simulation_state_static": (C.c_int, [_d3, C.c_int64, C.POINTER(C.c_int8), _i3, _d3, _vp]),
 }

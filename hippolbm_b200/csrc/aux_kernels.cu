@@ -3,8 +3,10 @@
 // obstacle tests and the initial populations round exactly like the reference's.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "aux_kernels.cuh"
-#include "lbm_step.cuh"
+#include "lbm_step_tma.cuh"
 
 namespace hlbm {
 
@@ -22,6 +24,95 @@ __global__ void k_set_distribution(S* f, int64_t stride, int nx, int ny, int lo0
     const double v = value * (1.0 / D3Q19::wden[I]);
     f[I * stride + idx] = Codec<S, R>::template enc<I>(R(v), p);
   });
+}
+
+// init_double_couette (double_couette.hpp:25-49, init_double_couette.cu:74-100): equilibrium of
+// u = Uc - dU * g at every real node, g its global index along `dim`; FP64 in the reference's
+// operation order, then stored.
+template <typename S, typename R>
+__global__ void k_double_couette(S* f, const StepPlan p, int dim, double ucx, double ucy, double ucz, double dux,
+                                 double duy, double duz) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int z = blockIdx.z;
+  if (x >= p.nx) return;
+  const int64_t idx = ((int64_t)z * p.ny + y) * p.nx + x;
+  const double g = dim == 0 ? double(x) : (dim == 1 ? double(y) : double(z));
+  const double ux = ucx - dux * g, uy = ucy - duy * g, uz = ucz - duz * g;
+  const double u_squ = ux * ux + uy * uy + uz * uz;
+  Unroll<0, Q>::run([&]<int I>() {
+    const double eu = ux * double(D3Q19::ex[I]) + uy * double(D3Q19::ey[I]) + uz * double(D3Q19::ez[I]);
+    const double w = 1.0 / D3Q19::wden[I];
+    const double v = 1. * w * (1. + 3. * eu + 4.5 * eu * eu - 1.5 * u_squ);
+    f[I * p.stride + idx] = Codec<S, R>::template enc<I>(R(v), p);
+  });
+}
+
+cudaError_t launch_double_couette(int prec, void* f, const StepPlan& p, int dim, const double uc[3],
+                                  const double du[3], cudaStream_t s) {
+  dim3 block(128), grid((p.nx + 127) / 128, p.ny, p.nz);
+  switch (prec) {
+    case 2:
+      k_double_couette<float, float><<<grid, block, 0, s>>>(static_cast<float*>(f), p, dim, uc[0], uc[1], uc[2],
+                                                            du[0], du[1], du[2]);
+      break;
+    case 3:
+      k_double_couette<__half, float><<<grid, block, 0, s>>>(static_cast<__half*>(f), p, dim, uc[0], uc[1], uc[2],
+                                                             du[0], du[1], du[2]);
+      break;
+    case 4:
+      k_double_couette<__nv_bfloat16, float><<<grid, block, 0, s>>>(static_cast<__nv_bfloat16*>(f), p, dim, uc[0],
+                                                                    uc[1], uc[2], du[0], du[1], du[2]);
+      break;
+    default:
+      k_double_couette<double, double><<<grid, block, 0, s>>>(static_cast<double*>(f), p, dim, uc[0], uc[1], uc[2],
+                                                              du[0], du[1], du[2]);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ zero-gradient outlet pass
+// The pass over one face of lattice m of a descriptor array (lbm_step.cuh: zero_gradient_node),
+// run before each step that pulls from f[cur ^ parity].
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_zero_gradient(const LatticeDesc* __restrict__ lats, int m, int face,
+                                                       int parity) {
+  __shared__ StepPlan sp;
+  const LatticeDesc L = lats[m];
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(L.plan);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sp);
+  for (int w = threadIdx.x; w < int(sizeof(StepPlan) / 4); w += blockDim.x) dst[w] = src[w];
+  __syncthreads();
+  const StepPlan& p = sp;
+  S* fin = static_cast<S*>(L.f[L.cur ^ parity]);
+  const int axis = face / 2;
+  const int na = axis == 0 ? p.ny : p.nx, nb = axis == 2 ? p.ny : p.nz;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < int64_t(na) * nb;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int a = int(k % na), b = int(k / na);
+    switch (face) {
+      case 0: zero_gradient_node<S, R, 0>(fin, L.flags, p, a, b); break;
+      case 1: zero_gradient_node<S, R, 1>(fin, L.flags, p, a, b); break;
+      case 2: zero_gradient_node<S, R, 2>(fin, L.flags, p, a, b); break;
+      case 3: zero_gradient_node<S, R, 3>(fin, L.flags, p, a, b); break;
+      case 4: zero_gradient_node<S, R, 4>(fin, L.flags, p, a, b); break;
+      default: zero_gradient_node<S, R, 5>(fin, L.flags, p, a, b); break;
+    }
+  }
+}
+
+cudaError_t launch_zero_gradient(int prec, const LatticeDesc* lats, int m, int face, int parity, const int n[3],
+                                 cudaStream_t s) {
+  const int axis = face / 2;
+  const int64_t nodes = int64_t(axis == 0 ? n[1] : n[0]) * (axis == 2 ? n[1] : n[2]);
+  const int blocks = int(std::min<int64_t>((nodes + 255) / 256, 4 * 148));
+  switch (prec) {
+    case 2: k_zero_gradient<float, float><<<blocks, 256, 0, s>>>(lats, m, face, parity); break;
+    case 3: k_zero_gradient<__half, float><<<blocks, 256, 0, s>>>(lats, m, face, parity); break;
+    case 4: k_zero_gradient<__nv_bfloat16, float><<<blocks, 256, 0, s>>>(lats, m, face, parity); break;
+    default: k_zero_gradient<double, double><<<blocks, 256, 0, s>>>(lats, m, face, parity); break;
+  }
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ obstacles
@@ -362,6 +453,79 @@ cudaError_t launch_wall_force(int prec, const void* fpost, const int8_t* flags, 
   const int nb = stats_blocks(p.ncell);
   HLBM_PREC_DISPATCH(prec, (k_wall_force<S, R><<<nb, 256, 0, s>>>(static_cast<const S*>(fpost), flags, partials, p)));
   k_fold_sums<<<1, 256, 0, s>>>(partials, nb, out4);
+  return cudaGetLastError();
+}
+
+// plane_velocity_profile (plane_velocity_profile.cu:64-90, 179-260): per plane normal to `dim`,
+// the sum, count, minimum and maximum over fluid nodes of |ratio * u| (FP64, u from the same
+// macro arithmetic as the statistics).  One block per plane, fixed thread-to-node assignment and a
+// fixed-order reduction: deterministic.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_plane_profile(const S* __restrict__ f, const int8_t* __restrict__ flags,
+                                                       const StepPlan p, int dim, double ratio,
+                                                       double* __restrict__ out) {
+  const int plane = blockIdx.x;
+  const int64_t nplane = dim == 0 ? int64_t(p.ny) * p.nz : (dim == 1 ? int64_t(p.nx) * p.nz : int64_t(p.nx) * p.ny);
+  double sum = 0.0, cnt = 0.0, vmin = 1.79769313486231570815e+308, vmax = -1.79769313486231570815e+308;
+  for (int64_t k = threadIdx.x; k < nplane; k += blockDim.x) {
+    int64_t idx;
+    if (dim == 2) {
+      idx = int64_t(plane) * p.nx * p.ny + k;
+    } else if (dim == 1) {
+      const int64_t z = k / p.nx, x = k - z * p.nx;
+      idx = (z * p.ny + plane) * p.nx + x;
+    } else {
+      idx = k * p.nx + plane;
+    }
+    if (flags[idx] != FLAG_FLUID) continue;
+    double v[Q];
+    Unroll<0, Q>::run([&]<int I>() { v[I] = double(Codec<S, R>::template dec<I>(f[I * p.stride + idx], p)); });
+    double rho, ux, uy, uz;
+    macro<double, true>(v, rho, ux, uy, uz);
+    const double ax = ratio * ux, ay = ratio * uy, az = ratio * uz;
+    const double n = sqrt(ax * ax + ay * ay + az * az);
+    sum += n;
+    cnt += 1.0;
+    vmin = n < vmin ? n : vmin;
+    vmax = n > vmax ? n : vmax;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, off);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    const double a = __shfl_down_sync(0xffffffffu, vmin, off);
+    const double b = __shfl_down_sync(0xffffffffu, vmax, off);
+    vmin = a < vmin ? a : vmin;
+    vmax = b > vmax ? b : vmax;
+  }
+  __shared__ double sh[4][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    sh[0][warp] = sum;
+    sh[1][warp] = cnt;
+    sh[2][warp] = vmin;
+    sh[3][warp] = vmax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = sh[0][0], c = sh[1][0], lo = sh[2][0], hi = sh[3][0];
+    for (int w = 1; w < int(blockDim.x >> 5); w++) {
+      a += sh[0][w];
+      c += sh[1][w];
+      lo = sh[2][w] < lo ? sh[2][w] : lo;
+      hi = sh[3][w] > hi ? sh[3][w] : hi;
+    }
+    out[4 * plane + 0] = a;
+    out[4 * plane + 1] = c;
+    out[4 * plane + 2] = lo;
+    out[4 * plane + 3] = hi;
+  }
+}
+
+cudaError_t launch_plane_profile(int prec, const void* f, const int8_t* flags, const StepPlan& p, int dim,
+                                 double ratio, double* out4n, cudaStream_t s) {
+  const int n = dim == 0 ? p.nx : (dim == 1 ? p.ny : p.nz);
+  HLBM_PREC_DISPATCH(prec, (k_plane_profile<S, R><<<n, 256, 0, s>>>(static_cast<const S*>(f), flags, p, dim, ratio,
+                                                                     out4n)));
   return cudaGetLastError();
 }
 

@@ -16,6 +16,11 @@ struct ObstacleDesc {
 
 cudaError_t launch_set_distribution(int prec, void* f, const StepPlan& p, const int lo[3], const int hi[3],
                                     double value, cudaStream_t s);
+cudaError_t launch_double_couette(int prec, void* f, const StepPlan& p, int dim, const double uc[3],
+                                  const double du[3], cudaStream_t s);
+struct LatticeDesc;
+cudaError_t launch_zero_gradient(int prec, const LatticeDesc* lats, int m, int face, int parity, const int n[3],
+                                 cudaStream_t s);
 cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], const int hi[3], double dx,
                              const ObstacleDesc& o, cudaStream_t s);
 int stats_blocks(int64_t ncell);
@@ -27,6 +32,8 @@ cudaError_t launch_moments(int prec, const void* f, const int8_t* flags, const S
                            double* out4, cudaStream_t s);
 cudaError_t launch_wall_force(int prec, const void* fpost, const int8_t* flags, const StepPlan& p, double* partials,
                               double* out4, cudaStream_t s);
+cudaError_t launch_plane_profile(int prec, const void* f, const int8_t* flags, const StepPlan& p, int dim,
+                                 double ratio, double* out4n, cudaStream_t s);
 cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s);
 cudaError_t launch_encode(int prec, void* f, const double* in, int dir, const StepPlan& p, cudaStream_t s);
 

@@ -37,7 +37,7 @@ int fail(int code, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(HLBM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-enum HookKind { H_PRE_BB, H_CAVITY, H_WALL_BB, H_POST_BB, H_NEUMANN, H_LID, H_SETDIST };
+enum HookKind { H_PRE_BB, H_CAVITY, H_WALL_BB, H_POST_BB, H_NEUMANN, H_LID, H_SETDIST, H_ZERO_GRADIENT };
 
 struct HookOp {
   int hook;
@@ -77,7 +77,7 @@ struct hlbm_ctx {
   double Fext[3], celerity, dtLB, nuth, nu, tau, avg_rho;
   int collision = 0;
   double mrt[8];
-  double rho0 = 1.0, scale = 1.0;
+  double rho0 = 1.0, scale = 1.0, u0[3] = {0.0, 0.0, 0.0};
   std::vector<HookOp> hooks;
   std::vector<ObstacleDesc> obstacles;
   void* f[2] = {nullptr, nullptr};
@@ -90,6 +90,7 @@ struct hlbm_ctx {
   cudaStream_t stream = nullptr;
   int phase = RAW;
   int variant = 0;  // step kernel variant (launch.cuh): kernel = variant % 2, occupancy = variant / 2
+  int rounding = 1;  // 16-bit storage: 1 stochastic rounding (default), 0 round to nearest
   int64_t steps = 0;
   int64_t launches = 0;
   int64_t ncell = 0, stride = 0;
@@ -101,6 +102,7 @@ struct hlbm_ctx {
   Tile* tiles_dev = nullptr;
   int* err_dev = nullptr;
   int ntiles = 0, tile_elems = 0, tma_stages = 0, tma_stages2 = 0, sms = 148;
+  hlbm_batch* batch = nullptr;  // the batch this lattice is a member of
 };
 
 namespace {
@@ -127,6 +129,13 @@ void base_plan(hlbm_ctx* c, StepPlan& p) {
   p.rho0 = c->rho0;
   p.scale = c->scale;
   p.inv_scale = 1.0 / c->scale;
+  const double uu = c->u0[0] * c->u0[0] + c->u0[1] * c->u0[1] + c->u0[2] * c->u0[2];
+  for (int i = 0; i < Q; i++) {  // feq_i(rho0, u0); u0 = 0 gives w_i * rho0
+    const double eu = D3Q19::ex[i] * c->u0[0] + D3Q19::ey[i] * c->u0[1] + D3Q19::ez[i] * c->u0[2];
+    p.dref[i] = float(W_OF(i) * c->rho0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu));
+  }
+  p.rounding = c->rounding;
+  p.seed = uint32_t(c->steps);
 }
 
 // the box {int(min / dx), int(max / dx)} of set_distribution / update_obstacles in real
@@ -249,6 +258,9 @@ int build_plan(hlbm_ctx* c) {
                       "post_bounce_back needs pre_bounce_back in pre_stream_bcs (it restores the saved populations)");
         op.kind = OP_POST_BB;
         op.face = 0;
+      } else if (h.kind == H_ZERO_GRADIENT) {
+        op.kind = OP_ZERO_GRADIENT;
+        op.face = h.face;
       } else {
         op.kind = h.kind == H_LID ? OP_LID : OP_ZOUHE;
         op.face = h.face;
@@ -274,8 +286,24 @@ int build_plan(hlbm_ctx* c) {
   return HLBM_OK;
 }
 
+// the zero-gradient outlet passes of a plan: every pull of a step (or a read-out) sees them
+cudaError_t outlet_passes(int prec, const StepPlan& p, const LatticeDesc* descs, int m, int parity, const int n[3],
+                          cudaStream_t s, int64_t& launches) {
+  for (int o = 0; o < p.nops; o++) {
+    if (p.ops[o].kind != OP_ZERO_GRADIENT) continue;
+    launches++;
+    if (cudaError_t e = launch_zero_gradient(prec, descs, m, p.ops[o].face, parity, n, s)) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fout, int variant) {
+  c->plan.seed = uint32_t(c->steps);  // the step number salts the stochastic rounding
   const StepPlan& p = c->plan;
+  if (mode != MODE_PROLOGUE)  // the descriptor holds f[0], f[1] with cur = 0
+    if (cudaError_t e = outlet_passes(c->precision, p, c->desc_dev, 0, fin == c->f[0] ? 0 : 1, c->n, c->stream,
+                                      c->launches))
+      return e;
   const int walls = p.walls;
   TmaArgs t;
   t.desc = c->desc_dev;
@@ -288,6 +316,7 @@ cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fo
   t.parity = (fin == c->f[0]) ? 0 : 1;
   t.err = c->err_dev;
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
+  t.seed = c->steps;
   c->launches++;
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
@@ -437,6 +466,7 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
 
 int hlbm_destroy(hlbm_ctx* c) {
   if (!c) return HLBM_OK;
+  if (c->batch) hlbm_batch_remove(c->batch, c);  // a batch never keeps a destroyed member
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->f[0]);
@@ -510,11 +540,10 @@ int hlbm_collision(hlbm_ctx* c, int32_t kind, const double* rates8) {
   return HLBM_OK;
 }
 
-int hlbm_storage_scale(hlbm_ctx* c, double rho0, double scale) {
-  if (!c || !(scale > 0)) return fail(HLBM_EINVAL, "hlbm_storage_scale: scale must be > 0");
+// re-encode the current state under new deviation parameters
+static int set_storage(hlbm_ctx* c, double rho0, double scale, const double u0[3]) {
   int rc = make_raw(c);
   if (rc) return rc;
-  // re-encode the current state under the new deviation parameters
   std::vector<double> host;
   if (c->precision == HLBM_F16 || c->precision == HLBM_BF16) {
     host.resize(size_t(Q) * c->ncell);
@@ -522,8 +551,28 @@ int hlbm_storage_scale(hlbm_ctx* c, double rho0, double scale) {
   }
   c->rho0 = rho0;
   c->scale = scale;
+  for (int d = 0; d < 3; d++) c->u0[d] = u0[d];
   c->plan_dirty = true;
   if (!host.empty()) return hlbm_put_populations(c, host.data());
+  return HLBM_OK;
+}
+
+int hlbm_storage_scale(hlbm_ctx* c, double rho0, double scale) {
+  if (!c || !(scale > 0)) return fail(HLBM_EINVAL, "hlbm_storage_scale: scale must be > 0");
+  return set_storage(c, rho0, scale, c->u0);
+}
+
+int hlbm_storage_reference(hlbm_ctx* c, double rho0, const double u0[3]) {
+  if (!c || !u0) return fail(HLBM_EINVAL, "hlbm_storage_reference: NULL argument");
+  if (!(std::fabs(u0[0]) < 0.5 && std::fabs(u0[1]) < 0.5 && std::fabs(u0[2]) < 0.5))
+    return fail(HLBM_EINVAL, "hlbm_storage_reference: |u0| components must be below 0.5 (lattice units)");
+  return set_storage(c, rho0, c->scale, u0);
+}
+
+int hlbm_storage_rounding(hlbm_ctx* c, int32_t mode) {
+  if (!c || (mode != 0 && mode != 1)) return fail(HLBM_EINVAL, "hlbm_storage_rounding: mode must be 0 or 1");
+  c->rounding = mode;
+  c->plan_dirty = true;
   return HLBM_OK;
 }
 
@@ -537,6 +586,23 @@ int hlbm_set_distribution(hlbm_ctx* c, double value, const double* bounds6, int3
   base_plan(c, p);
   c->launches++;
   HLBM_CK(launch_set_distribution(c->precision, c->f[c->cur], p, lo, hi, value, c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_init_double_couette(hlbm_ctx* c, const double U[3], int32_t dim) {
+  if (!c || !U) return fail(HLBM_EINVAL, "hlbm_init_double_couette: NULL argument");
+  if (dim < 0 || dim > 2)
+    return fail(HLBM_EINVAL, "[init_double_couette] Please, select a valid dimension \"X\", \"Y\", or \"Z\".");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = make_raw(c)) return rc;
+  double uc[3], du[3];
+  for (int d = 0; d < 3; d++) uc[d] = U[d] / c->celerity;  // init_double_couette.cu:77
+  const double half_span = 0.5 * (c->n[dim] - 1);
+  for (int d = 0; d < 3; d++) du[d] = uc[d] / half_span;
+  StepPlan p;
+  base_plan(c, p);
+  c->launches++;
+  HLBM_CK(launch_double_couette(c->precision, c->f[c->cur], p, dim, uc, du, c->stream));
   return HLBM_OK;
 }
 
@@ -654,6 +720,8 @@ static int plane_hooks(hlbm_ctx* c, int32_t hook, int kind, const double U[3], c
     return fail(HLBM_EINVAL, std::string(name) + ": bad argument");
   for (int i = 0; i < nreg; i++) {  // check_traversal_allowed (grid_region.hpp:381-387)
     if (regions[i] < 0 || regions[i] > 5) return fail(HLBM_EINVAL, std::string(name) + ": Traversal name not allowed");
+    if (kind == H_ZERO_GRADIENT && c->n[regions[i] / 2] < 2)  // the interior neighbour must exist
+      return fail(HLBM_EINVAL, std::string(name) + ": the face needs at least two nodes along its normal");
     add_hook(c, HookOp{hook, kind, regions[i], {U[0], U[1], U[2]}, 0, {0}});
   }
   return HLBM_OK;
@@ -665,6 +733,11 @@ int hlbm_neumann(hlbm_ctx* c, int32_t hook, const double U[3], const int32_t* re
 
 int hlbm_lid_driven_cavity(hlbm_ctx* c, int32_t hook, const double U[3], const int32_t* regions, int32_t nregions) {
   return plane_hooks(c, hook, H_LID, U, regions, nregions, "hlbm_lid_driven_cavity");
+}
+
+int hlbm_zero_gradient(hlbm_ctx* c, int32_t hook, const int32_t* regions, int32_t nregions) {
+  const double zero[3] = {0, 0, 0};
+  return plane_hooks(c, hook, H_ZERO_GRADIENT, zero, regions, nregions, "hlbm_zero_gradient");
 }
 
 int hlbm_start_set_distribution(hlbm_ctx* c, double value, const double bounds6[6]) {
@@ -856,6 +929,121 @@ int hlbm_put_flags(hlbm_ctx* c, const int8_t* in) {
   return HLBM_OK;
 }
 
+int hlbm_plane_velocity_profile(hlbm_ctx* c, int32_t dim, double* avg, double* vmin, double* vmax, int64_t* count) {
+  if (!c || dim < 0 || dim > 2) return fail(HLBM_EINVAL, "hlbm_plane_velocity_profile: dimension must be 0, 1 or 2");
+  if (int rc = set_device(c)) return rc;
+  void* s;
+  if (int rc = state_buffer(c, &s)) return rc;
+  const int n = c->n[dim];
+  double* dev = nullptr;
+  if (cudaMalloc(&dev, size_t(4) * n * sizeof(double)) != cudaSuccess)
+    return fail(HLBM_ENOMEM, "hlbm_plane_velocity_profile: no memory");
+  std::vector<double> host(size_t(4) * n);
+  StepPlan p;
+  base_plan(c, p);
+  c->launches++;
+  cudaError_t e = launch_plane_profile(c->precision, s, c->flags, p, dim, c->dx / c->dtLB, dev, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host.data(), dev, host.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(HLBM_ECUDA, std::string("hlbm_plane_velocity_profile: ") + cudaGetErrorString(e));
+  for (int i = 0; i < n; i++) {
+    const double sum = host[4 * i], cnt = host[4 * i + 1];
+    if (avg) avg[i] = cnt > 0 ? sum / cnt : 0.0;  // plane_velocity_profile.cu:206-212
+    if (vmin) vmin[i] = host[4 * i + 2];
+    if (vmax) vmax[i] = host[4 * i + 3];
+    if (count) count[i] = int64_t(cnt);
+  }
+  return HLBM_OK;
+}
+
+// ------------------------------------------------------------------ checkpoint / restore
+namespace {
+struct CheckpointHeader {
+  char magic[8];  // "HLBMCKP1"
+  int32_t version, precision;
+  int32_t n[3], periodic[3];
+  int32_t phase, rounding;
+  int64_t steps, ncell;
+  double rho0, scale, u0[3];
+};
+constexpr char CKPT_MAGIC[8] = {'H', 'L', 'B', 'M', 'C', 'K', 'P', '1'};
+int64_t checkpoint_bytes(const hlbm_ctx* c) {
+  return int64_t(sizeof(CheckpointHeader)) + c->ncell + int64_t(Q) * c->ncell * int64_t(elem_size(c->precision));
+}
+}  // namespace
+
+int hlbm_checkpoint_bytes(hlbm_ctx* c, int64_t* bytes) {
+  if (!c || !bytes) return fail(HLBM_EINVAL, "hlbm_checkpoint_bytes: NULL argument");
+  *bytes = checkpoint_bytes(c);
+  return HLBM_OK;
+}
+
+int hlbm_checkpoint_save(hlbm_ctx* c, void* host, int64_t bytes) {
+  if (!c || !host) return fail(HLBM_EINVAL, "hlbm_checkpoint_save: NULL argument");
+  if (bytes < checkpoint_bytes(c)) return fail(HLBM_EINVAL, "hlbm_checkpoint_save: buffer too small");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = check_device_error(c)) return rc;
+  if (c->phase == MATER) c->phase = POSTCOL;  // f[cur] holds the carried state in every phase
+  CheckpointHeader h{};
+  std::memcpy(h.magic, CKPT_MAGIC, 8);
+  h.version = 1;
+  h.precision = c->precision;
+  for (int d = 0; d < 3; d++) {
+    h.n[d] = c->n[d];
+    h.periodic[d] = c->periodic[d];
+  }
+  h.phase = c->phase;
+  h.rounding = c->rounding;
+  h.steps = c->steps;
+  h.ncell = c->ncell;
+  h.rho0 = c->rho0;
+  h.scale = c->scale;
+  for (int d = 0; d < 3; d++) h.u0[d] = c->u0[d];
+  unsigned char* out = static_cast<unsigned char*>(host);
+  std::memcpy(out, &h, sizeof(h));
+  out += sizeof(h);
+  const size_t n = size_t(c->ncell), es = elem_size(c->precision);
+  HLBM_CK(cudaMemcpyAsync(out, c->flags, n, cudaMemcpyDeviceToHost, c->stream));
+  out += n;
+  HLBM_CK(cudaMemcpy2DAsync(out, n * es, c->f[c->cur], size_t(c->stride) * es, n * es, Q, cudaMemcpyDeviceToHost,
+                            c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  return HLBM_OK;
+}
+
+int hlbm_checkpoint_load(hlbm_ctx* c, const void* host, int64_t bytes) {
+  if (!c || !host) return fail(HLBM_EINVAL, "hlbm_checkpoint_load: NULL argument");
+  if (bytes < int64_t(sizeof(CheckpointHeader))) return fail(HLBM_EINVAL, "hlbm_checkpoint_load: truncated header");
+  CheckpointHeader h;
+  std::memcpy(&h, host, sizeof(h));
+  if (std::memcmp(h.magic, CKPT_MAGIC, 8) != 0 || h.version != 1)
+    return fail(HLBM_EINVAL, "hlbm_checkpoint_load: not a checkpoint of this library");
+  if (h.precision != c->precision) return fail(HLBM_EINVAL, "hlbm_checkpoint_load: precision differs");
+  for (int d = 0; d < 3; d++)
+    if (h.n[d] != c->n[d] || h.periodic[d] != c->periodic[d])
+      return fail(HLBM_EDOMAIN, "hlbm_checkpoint_load: lattice shape or periodicity differs");
+  if (h.phase != RAW && h.phase != POSTCOL) return fail(HLBM_EINVAL, "hlbm_checkpoint_load: bad phase");
+  if (bytes < checkpoint_bytes(c)) return fail(HLBM_EINVAL, "hlbm_checkpoint_load: truncated data");
+  if (int rc = set_device(c)) return rc;
+  const unsigned char* in = static_cast<const unsigned char*>(host) + sizeof(h);
+  const size_t n = size_t(c->ncell), es = elem_size(c->precision);
+  HLBM_CK(cudaMemcpyAsync(c->flags, in, n, cudaMemcpyHostToDevice, c->stream));
+  in += n;
+  HLBM_CK(cudaMemcpy2DAsync(c->f[c->cur], size_t(c->stride) * es, in, n * es, n * es, Q, cudaMemcpyHostToDevice,
+                            c->stream));
+  HLBM_CK(cudaStreamSynchronize(c->stream));
+  c->phase = h.phase;
+  c->steps = h.steps;
+  c->rounding = h.rounding;
+  c->rho0 = h.rho0;  // the stored deviations are relative to these
+  c->scale = h.scale;
+  for (int d = 0; d < 3; d++) c->u0[d] = h.u0[d];
+  c->plan_dirty = true;
+  return HLBM_OK;
+}
+
 int hlbm_info(hlbm_ctx* c, int64_t info[8]) {
   if (!c || !info) return fail(HLBM_EINVAL, "hlbm_info: NULL argument");
   info[0] = c->n[0];
@@ -1026,6 +1214,8 @@ int batch_refresh_descs(hlbm_batch* b) {
     descs[m].flags = c->flags;
     descs[m].cur = c->cur;
     descs[m].prologue = c->phase == RAW ? 1 : 0;
+    descs[m].step[0] = uint32_t(c->steps);  // batched launches start at parity 0
+    descs[m].step[1] = uint32_t(c->steps + 1);
   }
   if (!descs.empty())
     HLBM_CK(cudaMemcpyAsync(b->desc_dev, descs.data(), descs.size() * sizeof(LatticeDesc), cudaMemcpyHostToDevice,
@@ -1046,6 +1236,15 @@ cudaError_t batch_launch(hlbm_batch* b, int parity) {
   t.parity = parity;
   t.err = b->err_dev;
   t.grid = std::min(b->ntiles, b->sms * t.ctas_per_sm);
+  t.seed = -1;
+  t.ndesc = int(b->members.size());
+  for (size_t m = 0; m < b->members.size(); m++) {  // members that pull this launch (not fresh)
+    hlbm_ctx* c = b->members[m];
+    if (c->phase == RAW) continue;
+    if (cudaError_t e = outlet_passes(b->precision, c->plan, b->desc_dev, int(m), parity, c->n, b->stream,
+                                      b->launches))
+      return e;
+  }
   StepPlan dummy;
   std::memset(&dummy, 0, sizeof(dummy));
   b->launches++;
@@ -1084,11 +1283,12 @@ int hlbm_batch_add(hlbm_batch* b, hlbm_ctx* c) {
   if (!b || !c) return fail(HLBM_EINVAL, "hlbm_batch_add: NULL argument");
   if (c->precision != b->precision || c->device != b->device)
     return fail(HLBM_EINVAL, "hlbm_batch_add: lattice precision or device differs from the batch");
-  for (hlbm_ctx* m : b->members)
-    if (m == c) return fail(HLBM_EINVAL, "hlbm_batch_add: lattice already in the batch");
+  if (c->batch == b) return fail(HLBM_EINVAL, "hlbm_batch_add: lattice already in the batch");
+  if (c->batch) return fail(HLBM_EINVAL, "hlbm_batch_add: lattice is a member of another batch");
   if (b->variant < 8 && (size_t(c->n[0]) * elem_size(c->precision)) % 16 != 0)
     return fail(HLBM_EPLAN, "hlbm_batch_add: the pipelined batch kernel needs nx * bytes per population % 16 == 0");
   b->members.push_back(c);
+  c->batch = b;
   b->dirty = true;
   return HLBM_OK;
 }
@@ -1097,7 +1297,9 @@ int hlbm_batch_remove(hlbm_batch* b, hlbm_ctx* c) {
   if (!b || !c) return fail(HLBM_EINVAL, "hlbm_batch_remove: NULL argument");
   for (size_t m = 0; m < b->members.size(); m++)
     if (b->members[m] == c) {
+      if (b->stream) cudaStreamSynchronize(b->stream);  // no batched launch still reads its memory
       b->members.erase(b->members.begin() + m);
+      c->batch = nullptr;
       b->dirty = true;
       return HLBM_OK;
     }
@@ -1193,10 +1395,13 @@ int hlbm_batch_info(hlbm_batch* b, int64_t info[6]) {
   return HLBM_OK;
 }
 
+void* hlbm_batch_stream(hlbm_batch* b) { return b ? (void*)b->stream : nullptr; }
+
 int hlbm_batch_destroy(hlbm_batch* b) {
   if (!b) return HLBM_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  for (hlbm_ctx* c : b->members) c->batch = nullptr;
   batch_drop_graph(b);
   cudaFree(b->desc_dev);
   cudaFree(b->tiles_dev);

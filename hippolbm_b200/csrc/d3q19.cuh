@@ -29,7 +29,7 @@ struct PlaneBB {
 };
 
 // Step plan: the node-local form of the operator lists of one deck.
-enum OpKind : int32_t { OP_POST_BB = 0, OP_ZOUHE = 1, OP_LID = 2, OP_SETDIST = 3 };
+enum OpKind : int32_t { OP_POST_BB = 0, OP_ZOUHE = 1, OP_LID = 2, OP_SETDIST = 3, OP_ZERO_GRADIENT = 4 };
 constexpr int MAX_PLANE_OPS = 16;
 constexpr int MAX_CAVITY = 4;
 constexpr int MAX_SETS = 8;
@@ -60,8 +60,11 @@ struct StepPlan {
   double F[3];
   double mrt[8];      // s_e, s_eps, s_q, s_pi, s_m, w_eps, w_epsj, w_xx
   double cav[6][MAX_CAVITY][5];
-  double rho0;        // reference density of the deviation storage (f - w * rho0)
+  double rho0;        // reference density of the deviation storage
   double scale, inv_scale;  // deviation storage scale
+  float dref[Q];      // 16-bit storage keeps (f_i - dref_i) * scale; dref_i = feq_i(rho0, u0)
+  uint32_t seed;      // step number of the launch: salt of the stochastic rounding
+  int32_t rounding;   // 16-bit storage: 0 round to nearest, 1 stochastic rounding
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };

@@ -83,7 +83,7 @@ constexpr int NUM_VARIANTS = 8;
 
 // what the pipelined kernel needs besides the plan
 struct TmaArgs {
-  const LatticeDesc* desc = nullptr;
+  LatticeDesc* desc = nullptr;
   const Tile* tiles = nullptr;
   int ntiles = 0;
   int tile_elems = 0;  // elements of one direction in a stage
@@ -92,6 +92,8 @@ struct TmaArgs {
   int* err = nullptr;
   int grid = 0;
   int ctas_per_sm = 1;
+  long long seed = -1;  // step number of a single-lattice launch; -1: the descriptors' counters
+  int ndesc = 0;        // descriptors whose counters a batched launch advances
 };
 
 template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
@@ -100,7 +102,8 @@ cudaError_t launch_tma_t(const TmaArgs& a, cudaStream_t s) {
   const size_t smem = tma_smem_bytes(STAGES, a.tile_elems, sizeof(S));
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  kern<<<a.grid, TMA_THREADS, smem, s>>>(a.desc, a.tiles, a.ntiles, a.tile_elems, a.parity, a.err);
+  kern<<<a.grid, TMA_THREADS, smem, s>>>(a.desc, a.tiles, a.ntiles, a.tile_elems, a.parity, a.err, a.seed,
+                                                 a.ndesc);
   return cudaGetLastError();
 }
 
@@ -143,11 +146,11 @@ cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fo
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_tiles(const TmaArgs& a, int walls, int variant, cudaStream_t s) {
   if (variant == 9) {
-    if (walls) k_step_tiles<S, R, STRICT, true, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
-    else k_step_tiles<S, R, STRICT, false, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+    if (walls) k_step_tiles<S, R, STRICT, true, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
+    else k_step_tiles<S, R, STRICT, false, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
   } else {
-    if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
-    else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity);
+    if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
+    else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
   }
   return cudaGetLastError();
 }

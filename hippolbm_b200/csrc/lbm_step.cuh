@@ -54,32 +54,71 @@ template <>
 struct Codec<__half, float> {
   template <int I>
   __device__ static __forceinline__ float dec(__half s, const StepPlan& p) {
-    constexpr float w = 1.0f / D3Q19::wden[I];
-    return fmaf(__half2float(s), (float)p.inv_scale, w * (float)p.rho0);
+    return fmaf(__half2float(s), (float)p.inv_scale, p.dref[I]);
   }
   template <int I>
   __device__ static __forceinline__ __half enc(float v, const StepPlan& p) {
-    constexpr float w = 1.0f / D3Q19::wden[I];
-    return __float2half_rn((v - w * (float)p.rho0) * (float)p.scale);
+    return __float2half_rn((v - p.dref[I]) * (float)p.scale);
+  }
+  // stochastic rounding: the 13 FP32 mantissa bits below FP16's last bit get a random addend
+  // (the top 13 bits of r), then the value is truncated; Inf / NaN pass unchanged
+  template <int I>
+  __device__ static __forceinline__ __half enc_sr(float v, const StepPlan& p, uint32_t r) {
+    uint32_t b = __float_as_uint((v - p.dref[I]) * (float)p.scale);
+    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 19;
+    return __float2half_rz(__uint_as_float(b));
   }
 };
 template <>
 struct Codec<__nv_bfloat16, float> {
   template <int I>
   __device__ static __forceinline__ float dec(__nv_bfloat16 s, const StepPlan& p) {
-    constexpr float w = 1.0f / D3Q19::wden[I];
-    return fmaf(__bfloat162float(s), (float)p.inv_scale, w * (float)p.rho0);
+    return fmaf(__bfloat162float(s), (float)p.inv_scale, p.dref[I]);
   }
   template <int I>
   __device__ static __forceinline__ __nv_bfloat16 enc(float v, const StepPlan& p) {
-    constexpr float w = 1.0f / D3Q19::wden[I];
-    return __float2bfloat16_rn((v - w * (float)p.rho0) * (float)p.scale);
+    return __float2bfloat16_rn((v - p.dref[I]) * (float)p.scale);
+  }
+  // stochastic rounding: a random addend to the 16 discarded bits, then truncation
+  template <int I>
+  __device__ static __forceinline__ __nv_bfloat16 enc_sr(float v, const StepPlan& p, uint32_t r) {
+    uint32_t b = __float_as_uint((v - p.dref[I]) * (float)p.scale);
+    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 16;
+    return __ushort_as_bfloat16((unsigned short)(b >> 16));
   }
 };
 
 template <typename S>
 __device__ __forceinline__ S ld_stream(const S* p) {
   return __ldg(p);
+}
+
+// ------------------------------------------------------------------ storage rounding
+// With 16-bit storage a round-to-nearest store loses every update smaller than half a storage
+// quantum, so slowly evolving regions stagnate and the rounding error accumulates with one sign.
+// Stochastic rounding rounds up with probability equal to the discarded fraction: unbiased.  The
+// random bits are a hash of (node index, step number, direction) -- reproducible, and the same
+// for a lattice stepped alone or inside a batch.
+__device__ __forceinline__ uint32_t node_hash(int64_t idx, uint32_t seed) {
+  uint32_t h = uint32_t(idx) * 0x9E3779B1u ^ (seed * 0x85EBCA77u + 0x165667B1u);
+  h ^= h >> 16;  // integer finaliser (xor-shift / multiply rounds)
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h;
+}
+
+// bits for direction I: the high bits of the node hash times a per-direction odd constant
+template <int I>
+__device__ __forceinline__ uint32_t dir_bits(uint32_t h) {
+  constexpr uint32_t K = 0x9E3779B9u * (2u * I + 1u);
+  return h * K;
+}
+
+template <typename S>
+constexpr bool is_16bit() {
+  return sizeof(S) == 2;
 }
 
 // ------------------------------------------------------------------ compile-time loops
@@ -96,6 +135,22 @@ struct Unroll<N, N> {
   template <class F>
   __device__ static __forceinline__ void run(F&&) {}
 };
+
+// Stores the node's Q values to dst(I): stochastically rounded when the 16-bit tiers store the
+// carried state (MODE_PROLOGUE / MODE_FUSED with p.rounding), else rounded to nearest.  The
+// branch is taken once per node: selecting per value would make the compiler evaluate both
+// conversions for every value.
+template <typename S, typename R, int MODE, class Dst>
+__device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, int64_t idx, Dst&& dst) {
+  if constexpr (is_16bit<S>() && MODE != MODE_FINISH) {
+    if (p.rounding) {
+      const uint32_t h = node_hash(idx, p.seed);
+      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc_sr<I>(v[I], p, dir_bits<I>(h))); });
+      return;
+    }
+  }
+  Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc<I>(v[I], p)); });
+}
 
 template <typename R, int I>
 __device__ __forceinline__ constexpr R weight() {
@@ -408,6 +463,51 @@ __device__ __forceinline__ void post_bb(R (&v)[Q], const S* __restrict__ fin, in
   });
 }
 
+// The streamed (pulled) value of direction I at node (x, y, z): the post-collision population of
+// the upstream node, or the node's own opposite one where the upstream node is outside a
+// non-periodic face or (wall_bounce_back active) a wall.
+template <typename S, typename R, int I>
+__device__ __forceinline__ R pull_value(const S* __restrict__ fin, const int8_t* __restrict__ flags,
+                                        const StepPlan& p, int x, int y, int z) {
+  constexpr int O = D3Q19::opp(I);
+  int sx = x - D3Q19::ex[I], sy = y - D3Q19::ey[I], sz = z - D3Q19::ez[I];
+  bool out = false;
+  if (sx < 0 || sx >= p.nx) { if (p.periodic[0]) sx = sx < 0 ? sx + p.nx : sx - p.nx; else out = true; }
+  if (sy < 0 || sy >= p.ny) { if (p.periodic[1]) sy = sy < 0 ? sy + p.ny : sy - p.ny; else out = true; }
+  if (sz < 0 || sz >= p.nz) { if (p.periodic[2]) sz = sz < 0 ? sz + p.nz : sz - p.nz; else out = true; }
+  const int64_t self = ((int64_t)z * p.ny + y) * p.nx + x;
+  const int64_t src = ((int64_t)sz * p.ny + sy) * p.nx + sx;
+  if (!out && p.walls && I != 0 && flags[src] == FLAG_WALL) out = true;
+  return out ? Codec<S, R>::template dec<O>(ld_stream(fin + O * p.stride + self), p)
+             : Codec<S, R>::template dec<I>(ld_stream(fin + I * p.stride + src), p);
+}
+
+// zero_gradient (no reference counterpart): on face F the populations that enter from outside
+// (the directions post_bounce_back restores) take the streamed values of the interior neighbour
+// one node inside along the face normal.  It runs before the step as a pass over the face: a
+// population I entering at a face node reaches the node by on-node bounce-back, i.e. from the
+// node's own outgoing slot opp(I), which nothing else reads (its streaming target is outside the
+// lattice).  The pass writes the neighbour's streamed value there, so the step kernels need no
+// outlet code.  It reads only entering slots and interior nodes' slots, never the slots it
+// writes.  (a, b) are the node's coordinates along the face's two other axes, in x, y, z order.
+template <typename S, typename R, int F>
+__device__ __forceinline__ void zero_gradient_node(S* __restrict__ fin, const int8_t* __restrict__ flags,
+                                                   const StepPlan& p, int a, int b) {
+  constexpr int axis = F / 2;
+  const int c = (F & 1) ? (axis == 0 ? p.nx : (axis == 1 ? p.ny : p.nz)) - 1 : 0;
+  const int m = (F & 1) ? c - 1 : c + 1;  // interior neighbour along the normal
+  const int x = axis == 0 ? c : a, y = axis == 1 ? c : (axis == 0 ? a : b), z = axis == 2 ? c : b;
+  const int64_t self = ((int64_t)z * p.ny + y) * p.nx + x;
+  if (flags[self] != FLAG_FLUID) return;  // like the neumann / lid operators: fluid nodes only
+  const int mx = axis == 0 ? m : x, my = axis == 1 ? m : y, mz = axis == 2 ? m : z;
+  Unroll<0, 5>::run([&]<int K>() {
+    constexpr int I = PlaneBB::post[F][K];
+    constexpr int O = D3Q19::opp(I);
+    const R v = pull_value<S, R, I>(fin, flags, p, mx, my, mz);
+    fin[O * p.stride + self] = Codec<S, R>::template enc<O>(v, p);
+  });
+}
+
 template <typename S, typename R>
 __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, int64_t idx, int x, int y, int z,
                                           int8_t flag, const StepPlan& p) {
@@ -417,6 +517,7 @@ __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, 
       post_bb<S, R>(v, fin, idx, x, y, z, p);
       continue;
     }
+    if (op.kind == OP_ZERO_GRADIENT) continue;  // applied by the outlet pass before the step
     if (flag != FLAG_FLUID) continue;  // neuman / lid functors act on fluid nodes only
     bool hit;
     switch (op.face) {
@@ -511,7 +612,7 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
     }
     if (flag == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
   }
-  Unroll<0, Q>::run([&]<int I>() { fout[I * p.stride + idx] = Codec<S, R>::template enc<I>(v[I], p); });
+  store_node<S, R, MODE>(v, p, idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
 }
 
 // ------------------------------------------------------------------ the step kernel

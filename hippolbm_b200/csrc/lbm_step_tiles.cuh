@@ -12,13 +12,17 @@ namespace hlbm {
 
 template <typename S, typename R, bool STRICT, bool WALLS, int MINB>
 __global__ void __launch_bounds__(256, MINB)
-    k_step_tiles(const LatticeDesc* __restrict__ lats, const Tile* __restrict__ tiles, int parity) {
+    k_step_tiles(LatticeDesc* __restrict__ lats, const Tile* __restrict__ tiles, int parity, long long seed,
+                 int ndesc) {
   __shared__ StepPlan splan;
+  advance_step_numbers(lats, ndesc, seed, parity, threadIdx.x, blockDim.x);
   const Tile tl = tiles[blockIdx.x];
   const LatticeDesc L = lats[tl.x];
   const uint32_t* src = reinterpret_cast<const uint32_t*>(L.plan);
   uint32_t* dst = reinterpret_cast<uint32_t*>(&splan);
   for (int w = threadIdx.x; w < int(sizeof(StepPlan) / 4); w += blockDim.x) dst[w] = src[w];
+  __syncthreads();
+  if (threadIdx.x == 0) splan.seed = launch_step_number(L, seed, parity);
   __syncthreads();
   const StepPlan& p = splan;
   const S* fin = static_cast<const S*>(L.f[L.cur ^ parity]);

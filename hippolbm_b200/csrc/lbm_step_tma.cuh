@@ -30,7 +30,21 @@ struct LatticeDesc {
   const int8_t* flags;
   int32_t cur;       // f[cur ^ parity] is read, the other written
   int32_t prologue;  // 1: the buffer read holds S_0; collide it without streaming (first step)
+  uint32_t step[2];  // step number of the next launch of each parity (batched launches)
+  uint32_t pad[2];
 };
+
+// Step number (rounding salt) of a launch: `seed` when the host passes one (>= 0), else the
+// lattice's own counter for this parity.  A batched launch also advances the counters: block 0
+// writes step[parity ^ 1] = step[parity] + 1, which no block of this launch reads.
+__device__ __forceinline__ uint32_t launch_step_number(const LatticeDesc& L, long long seed, int parity) {
+  return seed >= 0 ? uint32_t(seed) : L.step[parity];
+}
+__device__ __forceinline__ void advance_step_numbers(LatticeDesc* lats, int ndesc, long long seed, int parity,
+                                                     int tid, int nthreads) {
+  if (seed >= 0 || blockIdx.x != 0) return;
+  for (int m = tid; m < ndesc; m += nthreads) lats[m].step[parity ^ 1] = lats[m].step[parity] + 1u;
+}
 
 // tile: {lattice, z, y0, rows}
 using Tile = int4;
@@ -148,8 +162,8 @@ __device__ __forceinline__ void issue_direction(const LatticeDesc& L, const Step
 
 template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
 __global__ void __launch_bounds__(TMA_THREADS, MINB)
-    k_step_tma(const LatticeDesc* __restrict__ lats, const Tile* __restrict__ tiles, int ntiles, int tile_elems,
-               int parity, int* __restrict__ err) {
+    k_step_tma(LatticeDesc* __restrict__ lats, const Tile* __restrict__ tiles, int ntiles, int tile_elems,
+               int parity, int* __restrict__ err, long long seed, int ndesc) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
   uint64_t* empty = full + STAGES;
@@ -192,6 +206,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
   // ------------------------------------------------------------------------ consumers
   const int ctid = threadIdx.x - 32;
   constexpr int NC = 32 * TMA_CONSUMER_WARPS;
+  advance_step_numbers(lats, ndesc, seed, parity, ctid, NC);
   int plan_of = -1;
   int k = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
@@ -202,6 +217,8 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
       const uint32_t* src = reinterpret_cast<const uint32_t*>(lats[tl.x].plan);
       uint32_t* dst = reinterpret_cast<uint32_t*>(splan);
       for (int w = ctid; w < int(sizeof(StepPlan) / 4); w += NC) dst[w] = src[w];
+      asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory");
+      if (ctid == 0) splan->seed = launch_step_number(lats[tl.x], seed, parity);
       asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory");
       plan_of = tl.x;
     }
@@ -261,7 +278,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
           Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
       }
       if (flag == FLAG_FLUID) collide<R, STRICT, 2>(v, p);
-      Unroll<0, Q>::run([&]<int I>() { fout[I * stride + idx] = Codec<S, R>::template enc<I>(v[I], p); });
+      store_node<S, R, MODE_FUSED>(v, p, idx, [&]<int I>(S s) { fout[I * stride + idx] = s; });
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s

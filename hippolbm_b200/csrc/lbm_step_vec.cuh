@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
       }
       if (fl[K] == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
     }
-    Unroll<0, Q>::run([&]<int I>() { c[I].template set<K>(Codec<S, R>::template enc<I>(v[I], p)); });
+    store_node<S, R, MODE>(v, p, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
   });
   Unroll<0, Q>::run([&]<int I>() { c[I].store(fout + I * p.stride + row + x0); });
 }

@@ -26,8 +26,8 @@ import yaml
 HOOK_OPERATORS = {
     "start_iteration": {"set_distribution"},
     "pre_stream_bcs": {"pre_bounce_back", "cavity_z_0", "cavity_z_l", "wall_bounce_back"},
-    "post_stream_bcs": {"post_bounce_back", "lid_driven_cavity", "neumann"},
-    "boundary_conditions": {"neumann", "lid_driven_cavity", "post_bounce_back"},
+    "post_stream_bcs": {"post_bounce_back", "lid_driven_cavity", "neumann", "zero_gradient"},
+    "boundary_conditions": {"neumann", "lid_driven_cavity", "post_bounce_back", "zero_gradient"},
 }
 PLANES = ["plan_yz_0", "plan_yz_l", "plan_xz_0", "plan_xz_l", "plan_xy_0", "plan_xy_l"]
 # traversal names accepted by neumann / lid_driven_cavity (neuman.cu:80-81)
@@ -68,6 +68,11 @@ class Case:
     steps: int = 100
     checks: list = dataclasses.field(default_factory=list)  # check_macro_quantities slots
     name: str = "case"
+    # init_double_couette slots (init_double_couette.cu:51-58): {"U": [...], "dimension": "Z"}
+    double_couette: dict | None = None
+    # the deck's `analysis` operators (config_analysis.msp) and run controls (`global:`)
+    analysis: list = dataclasses.field(default_factory=list)
+    run: dict = dataclasses.field(default_factory=dict)
 
     @property
     def nodes(self) -> tuple:
@@ -94,6 +99,7 @@ class Case:
         d = dict(d)
         for hook in HOOK_OPERATORS:
             d[hook] = [Op(name, dict(slots)) for name, slots in d.get(hook, [])]
+        d["analysis"] = [Op(a["name"], dict(a["slots"])) if isinstance(a, dict) else a for a in d.get("analysis", [])]
         for k in ("cell_dims", "bmin", "bmax", "periodic", "Fext"):
             d[k] = tuple(d[k])
         if d.get("mrt_rates") is not None:
@@ -245,6 +251,12 @@ def case_from_tree(tree: dict, name: str = "deck") -> Case:
         c.dt = float(s.get("dt", c.dt))
     # initial distributions: the `set_distributions` hook (config_initialize.msp:4,24).
     for op in _ops(tree.get("set_distributions")):
+        if op.name == "init_double_couette":
+            dim = str(op.slots.get("dimension", ""))
+            if dim not in ("X", "Y", "Z"):
+                raise DeckError('[init_double_couette] Please, select a valid dimension "X", "Y", or "Z".')
+            c.double_couette = {"U": list(_vec3(op.slots["U"], "init_double_couette.U")), "dimension": dim}
+            continue
         if op.name != "set_distribution":
             continue
         b = op.slots.get("bounds")
@@ -275,6 +287,14 @@ def case_from_tree(tree: dict, name: str = "deck") -> Case:
     c.boundary_conditions = _ops(tree.get("boundary_conditions"))
     g = tree.get("global", {}) or {}
     c.steps = int(_num(g.get("simulation_end_iteration", 100)))
+    # run controls, defaults of config_initialize.msp:36-43 and write_paraview.cpp:51-53
+    c.run = {"paraview_freq": int(_num(g.get("simulation_paraview_freq", -1))),
+             "analysis_freq": int(_num(g.get("simulation_analysis_freq", -1))),
+             "print_log_freq": int(_num(g.get("simulation_print_log_freq", 1))),
+             "display_paraview_first_timestep": bool(g.get("display_paraview_first_timestep", True)),
+             "output_directory": str(g.get("output_directory", "hippoLBMOutputDir"))}
+    ana = tree.get("analysis")
+    c.analysis = _ops(ana) if isinstance(ana, list) else []
     for op in _ops(tree.get("checker_op")):
         if op.name == "check_macro_quantities":
             c.checks.append(dict(op.slots))
@@ -333,3 +353,80 @@ def couette_case(n: int, tau: float, u_wall: float, steps: int, collision: str =
         periodic=tuple(periodic), tau=tau, nuth=(tau - 0.5) / 3.0, collision=collision,
         pre_stream_bcs=[Op("pre_bounce_back"), Op("cavity_z_l", {"U": [u_wall, 0.0, 0.0]})],
         post_stream_bcs=[Op("post_bounce_back")], steps=steps)
+
+
+# MRT rates with the stress-independent rates given explicitly and every other rate 1.0
+# (s_e = 1.19, s_eps = 1.4, s_q = 1.2, s_pi = s_m = 1.0; the equilibrium weights stay those of
+# mrt.hpp:43-47: w_eps = 0, w_epsj = -475/63, w_xx = 0).  The reference's own set keeps s_m = 1.98,
+# which drives the closed sphere channel unstable at tau = 0.56 within a hundred steps.
+MRT_RATES_REST_ONE = (1.19, 1.4, 1.2, 1.0, 1.0, 0.0, -475.0 / 63.0, 0.0)
+
+
+def sphere_channel_case(nodes=(1024, 256, 256), center=(256.0, 128.0, 128.0), radius: float = 24.0,
+                        tau: float = 0.56, u_in: float = 0.04, steps: int = 20000, collision: str = "mrt",
+                        mrt_rates=MRT_RATES_REST_ONE) -> Case:
+    """Flow past a sphere in a closed channel, lattice units (dx = dt = 1): bounce-back on the
+    sphere (wall_bounce_back) and on the y / z walls (plane bounce-back), a Zou/He velocity inlet
+    u_x = u_in on plan_yz_0 and a zero-gradient outlet on plan_yz_l.  Starts from rest (f = w)."""
+    nx, ny, nz = (int(v) for v in nodes)
+    return Case(
+        name=f"sphere_channel{nx}x{ny}x{nz}_{collision}", cell_dims=(nx - 1, ny - 1, nz - 1), bmin=(0.0,) * 3,
+        bmax=(float(nx - 1), float(ny - 1), float(nz - 1)), periodic=(False, False, False), tau=tau,
+        nuth=(tau - 0.5) / 3.0, collision=collision, mrt_rates=mrt_rates,
+        obstacles=[("ball", 0, (tuple(float(c) for c in center), float(radius)))],
+        pre_stream_bcs=[Op("pre_bounce_back"), Op("wall_bounce_back")],
+        post_stream_bcs=[Op("post_bounce_back")],
+        boundary_conditions=[Op("neumann", {"U": [float(u_in), 0.0, 0.0], "regions": ["plan_yz_0"]}),
+                             Op("zero_gradient", {"regions": ["plan_yz_l"]})],
+        steps=steps)
+
+
+def poiseuille_case(nodes, tau: float, force: float, steps: int, collision: str = "bgk") -> Case:
+    """Body-force driven channel: periodic in x and y, Zou/He zero-velocity walls (neumann U = 0)
+    on the z planes, force along x in lattice units."""
+    nx, ny, nz = (int(v) for v in nodes)
+    return Case(name=f"poiseuille{nx}x{ny}x{nz}_{collision}", cell_dims=(nx - 1, ny - 1, nz - 1), bmin=(0.0,) * 3,
+                bmax=(float(nx - 1), float(ny - 1), float(nz - 1)), periodic=(True, True, False), tau=tau,
+                nuth=(tau - 0.5) / 3.0, collision=collision, Fext=(float(force), 0.0, 0.0),
+                boundary_conditions=[Op("neumann", {"U": [0.0, 0.0, 0.0], "regions": ["plan_xy_0", "plan_xy_l"]})],
+                steps=steps)
+
+
+def lid_cavity_case(nodes, tau: float, u_lid: float, steps: int, collision: str = "bgk") -> Case:
+    """Closed box, plane bounce-back on every face and a lid moving along x on plan_xy_l."""
+    nx, ny, nz = (int(v) for v in nodes)
+    return Case(name=f"cavity{nx}x{ny}x{nz}_{collision}", cell_dims=(nx - 1, ny - 1, nz - 1), bmin=(0.0,) * 3,
+                bmax=(float(nx - 1), float(ny - 1), float(nz - 1)), periodic=(False, False, False), tau=tau,
+                nuth=(tau - 0.5) / 3.0, collision=collision,
+                pre_stream_bcs=[Op("pre_bounce_back")],
+                post_stream_bcs=[Op("post_bounce_back"),
+                                 Op("lid_driven_cavity", {"U": [float(u_lid), 0.0, 0.0], "regions": ["plan_xy_l"]})],
+                steps=steps)
+
+
+def mixed_batch_cases(count: int = 256, seed: int = 20261203, steps: int = 2000) -> list[Case]:
+    """Independent lattices drawn from `seed`: each axis length uniform on {32, 40, ..., 128}; the
+    case uniform among Couette (wall speed U[0.01, 0.08]), Poiseuille (body force U[1e-6, 1e-5]) and
+    lid-driven cavity (lid speed U[0.02, 0.1]); BGK or MRT; tau uniform in [0.55, 1.2]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    edges = np.arange(32, 129, 8)
+    out = []
+    for i in range(count):
+        nodes = tuple(int(v) for v in rng.choice(edges, size=3))
+        kind = str(rng.choice(["couette", "poiseuille", "cavity"]))
+        collision = str(rng.choice(["bgk", "mrt"]))
+        tau = float(rng.uniform(0.55, 1.2))
+        if kind == "couette":
+            c = couette_case(nodes[0], tau, float(rng.uniform(0.01, 0.08)), steps, collision)
+            nx, ny, nz = nodes
+            c.cell_dims = (nx - 1, ny - 1, nz - 1)
+            c.bmax = (float(nx - 1), float(ny - 1), float(nz - 1))
+        elif kind == "poiseuille":
+            c = poiseuille_case(nodes, tau, float(rng.uniform(1e-6, 1e-5)), steps, collision)
+        else:
+            c = lid_cavity_case(nodes, tau, float(rng.uniform(0.02, 0.1)), steps, collision)
+        c.name = f"m{i}_{kind}_{nodes[0]}x{nodes[1]}x{nodes[2]}_{collision}"
+        out.append(c)
+    return out

@@ -66,6 +66,9 @@ class Lattice:
         capi.check(L.hlbm_collision(h, 0 if case.collision == "bgk" else 1, rates))
         for value, bounds6 in case.init_distributions:
             capi.check(L.hlbm_set_distribution(h, value, capi.dvec(bounds6) if bounds6 else None, 0))
+        if case.double_couette:
+            dc = case.double_couette
+            capi.check(L.hlbm_init_double_couette(h, capi.dvec(dc["U"]), "XYZ".index(dc["dimension"])))
         capi.check(L.hlbm_init_obstacles(h))
         for kind, oid, prm in case.obstacles:
             if kind == "ball":
@@ -96,6 +99,9 @@ class Lattice:
                     regions = [PLANE_INDEX[r] for r in s["regions"]]
                     fn = L.hlbm_neumann if op.name == "neumann" else L.hlbm_lid_driven_cavity
                     capi.check(fn(h, hook, capi.dvec(s["U"]), capi.ivec(regions), len(regions)))
+                elif op.name == "zero_gradient":
+                    regions = [PLANE_INDEX[r] for r in s["regions"]]
+                    capi.check(L.hlbm_zero_gradient(h, hook, capi.ivec(regions), len(regions)))
                 elif op.name == "set_distribution":
                     b = s.get("bounds")
                     if b is None:
@@ -125,6 +131,26 @@ class Lattice:
         assert a.size == Q * self.ncell
         capi.check(self.L.hlbm_put_populations(self.h, a.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def checkpoint(self) -> np.ndarray:
+        """The carried state as one byte image (header, flags, populations as stored)."""
+        n = C.c_int64()
+        capi.check(self.L.hlbm_checkpoint_bytes(self.h, C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        capi.check(self.L.hlbm_checkpoint_save(self.h, buf.ctypes.data_as(C.c_void_p), n.value))
+        return buf
+
+    def restore(self, image: np.ndarray):
+        """Load an image from `checkpoint()` of a lattice built from the same deck."""
+        a = np.ascontiguousarray(image, dtype=np.uint8)
+        capi.check(self.L.hlbm_checkpoint_load(self.h, a.ctypes.data_as(C.c_void_p), a.size))
+        return self
+
+    def save_checkpoint(self, path: str):
+        self.checkpoint().tofile(path)
+
+    def load_checkpoint(self, path: str):
+        return self.restore(np.fromfile(path, dtype=np.uint8))
+
     def flags(self) -> np.ndarray:
         out = np.empty(self.ncell, dtype=np.int8)
         capi.check(self.L.hlbm_get_flags(self.h, out.ctypes.data_as(C.POINTER(C.c_int8))))
@@ -146,6 +172,19 @@ class Lattice:
         out = (C.c_double * 3)()
         capi.check(self.L.hlbm_simulation_state(self.h, out))
         return tuple(out)
+
+    def plane_velocity_profile(self, dimension: str = "Z"):
+        """plane_velocity_profile (plane_velocity_profile.cu:179-260): per plane normal to
+        `dimension`, (mean, min, max) of the velocity norm over fluid nodes and the fluid count."""
+        dim = {"X": 0, "Y": 1, "Z": 2}[dimension.upper()]
+        n = self.n[dim]
+        avg, vmin, vmax = np.empty(n), np.empty(n), np.empty(n)
+        cnt = np.empty(n, dtype=np.int64)
+        dp = C.POINTER(C.c_double)
+        capi.check(self.L.hlbm_plane_velocity_profile(self.h, dim, avg.ctypes.data_as(dp), vmin.ctypes.data_as(dp),
+                                                      vmax.ctypes.data_as(dp),
+                                                      cnt.ctypes.data_as(C.POINTER(C.c_int64))))
+        return avg, vmin, vmax, cnt
 
     def residual(self) -> float:
         out = C.c_double()
@@ -174,6 +213,17 @@ class Lattice:
         capi.check(self.L.hlbm_info(self.h, out))
         keys = ["nx", "ny", "nz", "precision", "steps", "launches", "bytes_per_population", "device"]
         return dict(zip(keys, list(out)))
+
+    def rounding(self, mode: str):
+        """16-bit storage rounding of the carried state: "stochastic" (default) or "nearest"."""
+        capi.check(self.L.hlbm_storage_rounding(self.h, {"nearest": 0, "stochastic": 1}[mode]))
+        return self
+
+    def storage_reference(self, rho0: float = 1.0, u0=(0.0, 0.0, 0.0)):
+        """16-bit tiers store f_i - feq_i(rho0, u0): a reference velocity near the flow's mean
+        velocity shrinks the stored deviations (and the rounding steps)."""
+        capi.check(self.L.hlbm_storage_reference(self.h, float(rho0), capi.dvec(u0)))
+        return self
 
     def tune(self, variant: int):
         capi.check(self.L.hlbm_tune(self.h, int(variant)))

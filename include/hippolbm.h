@@ -88,14 +88,27 @@ int hlbm_get_parameters(hlbm_ctx* ctx, double out[9]);
  * constants (mrt.hpp:43-47); s_nu = 1 / tau always. */
 int hlbm_collision(hlbm_ctx* ctx, int32_t kind, const double* rates8);
 
-/* Reduced-precision storage keeps (f_i - w_i * rho0) * scale (HLBM_F16: scale 1024 by
- * default, HLBM_BF16: 1).  No reference counterpart: part of the precision tiers. */
+/* Reduced-precision storage keeps (f_i - d_i) * scale with d_i = feq_i(rho0, u0), by default
+ * w_i * rho0 (u0 = 0, rho0 = 1; HLBM_F16: scale 1024, HLBM_BF16: 1).  hlbm_storage_reference sets
+ * a reference velocity u0 (lattice units): for a flow dominated by a known mean velocity the stored
+ * deviations, hence the rounding steps, shrink.  Both re-encode the current state.  No reference
+ * counterpart: part of the precision tiers. */
 int hlbm_storage_scale(hlbm_ctx* ctx, double rho0, double scale);
+int hlbm_storage_reference(hlbm_ctx* ctx, double rho0, const double u0[3]);
+/* Rounding of the 16-bit storage tiers when a step stores the state: 1 (the default) stochastic
+ * -- round up with probability equal to the discarded fraction, from a hash of (node, step
+ * number, direction), so results are reproducible and the same alone or in a batch -- or 0 round
+ * to nearest.  Read-outs always round to nearest.  No effect on FP64 / FP32. */
+int hlbm_storage_rounding(hlbm_ctx* ctx, int32_t mode);
 
 /* set_distribution (set_distribution.cu:69-109), applied now: f_i = value * w_i on the
  * nodes of the box {int(min/dx), int(max/dx)} clipped to the lattice, or on all nodes when
  * bounds6 is NULL.  do_update is accepted for compatibility (there are no ghost layers). */
 int hlbm_set_distribution(hlbm_ctx* ctx, double value, const double* bounds6, int32_t do_update);
+/* init_double_couette (init_double_couette.cu:74-100, double_couette.hpp:25-49): f = feq(rho = 1,
+ * u = U / c - dU * g) at every node, g the node's index along dim (0 x, 1 y, 2 z) and
+ * dU = (U / c) / (0.5 * (n[dim] - 1)): a linear profile from U at g = 0 to -U at the far face. */
+int hlbm_init_double_couette(hlbm_ctx* ctx, const double U[3], int32_t dim);
 
 /* obstacles: init_obstacles (init_obstacles.cpp), register_solid_ball
  * (register_solid_ball.cpp), register_solid_wall (register_solid_wall.cpp), register_quadrics
@@ -122,6 +135,11 @@ int hlbm_neumann(hlbm_ctx* ctx, int32_t hook, const double U[3], const int32_t* 
 int hlbm_lid_driven_cavity(hlbm_ctx* ctx, int32_t hook, const double U[3], const int32_t* regions,
                            int32_t nregions);
 int hlbm_start_set_distribution(hlbm_ctx* ctx, double value, const double bounds6[6]);
+/* zero_gradient outlet (no reference counterpart: the reference's "neumann" is a Zou/He velocity
+ * condition): on each listed plane, the populations entering from outside take the streamed values
+ * of the interior neighbour one node inside along the face normal.  post_stream_bcs or
+ * boundary_conditions. */
+int hlbm_zero_gradient(hlbm_ctx* ctx, int32_t hook, const int32_t* regions, int32_t nregions);
 
 /* nsteps iterations of compute_loop: macro_variables -> collision -> pre_stream_bcs ->
  * streaming (streaming.cu:68-118, asynchrone: false) -> post_stream_bcs ->
@@ -136,6 +154,14 @@ int hlbm_macro_variables(hlbm_ctx* ctx, double* rho, double* u);
  * nodes, FP64 on the device. */
 int hlbm_simulation_state(hlbm_ctx* ctx, double out[3]);
 
+/* plane_velocity_profile (plane_velocity_profile.cu:179-260): for each plane normal to dim (0 x,
+ * 1 y, 2 z), the mean, minimum and maximum over fluid nodes of |dx / dtLB * u| and the fluid node
+ * count, from the current state (FP64 on the device, deterministic).  Arrays hold n[dim] values;
+ * any may be NULL.  A plane without fluid nodes has mean 0, min DBL_MAX and max -DBL_MAX, as in the
+ * reference. */
+int hlbm_plane_velocity_profile(hlbm_ctx* ctx, int32_t dim, double* avg, double* vmin, double* vmax,
+                                int64_t* count);
+
 /* FP64 reductions on the device (no reference counterparts; used by the precision study and the
  * solve server).  hlbm_residual: relative L2 change of the velocity field since the previous call
  * on this context, sqrt(sum |u - u_prev|^2 / sum |u|^2) (HUGE_VAL on the first call; keeps an
@@ -149,6 +175,15 @@ int hlbm_wall_force(hlbm_ctx* ctx, double out[3]);
 /* populations of the current state (FP64, layout above); put replaces them */
 int hlbm_get_populations(hlbm_ctx* ctx, double* out);
 int hlbm_put_populations(hlbm_ctx* ctx, const double* in);
+/* Checkpoint / restore of the carried state (no reference counterpart).  The image holds a
+ * header (shape, precision, step count, storage parameters), the flag bytes and the populations
+ * exactly as stored (FP64 / FP32 / 16-bit), so a lattice restored into a context built from the
+ * same deck continues bit for bit in every tier.  The copies are asynchronous on the context's
+ * stream (pinned host memory makes them DMA transfers) and complete before the call returns. */
+int hlbm_checkpoint_bytes(hlbm_ctx* ctx, int64_t* bytes);
+int hlbm_checkpoint_save(hlbm_ctx* ctx, void* host, int64_t bytes);
+int hlbm_checkpoint_load(hlbm_ctx* ctx, const void* host, int64_t bytes);
+
 /* flag bytes: -1 fluid, -2 wall (enum.hpp:59-60) */
 int hlbm_get_flags(hlbm_ctx* ctx, int8_t* out);
 int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
@@ -180,7 +215,8 @@ void* hlbm_stream(hlbm_ctx* ctx);
  * direct pulls (at least 3 / 2 CTAs per SM), any lattice shape; 6 / 7 = the pipelined kernel
  * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0).  A
  * member that has not stepped yet takes its first step inside the batched launch.  While a
- * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.
+ * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.  A lattice
+ * belongs to at most one batch; hlbm_destroy of a member removes it from its batch first.
  * hlbm_batch_step(b, n) advances every member n steps. */
 typedef struct hlbm_batch hlbm_batch;
 int hlbm_batch_create(int32_t precision, int32_t device, hlbm_batch** out);
@@ -190,6 +226,8 @@ int hlbm_batch_step(hlbm_batch* b, int64_t nsteps);
 int hlbm_batch_tune(hlbm_batch* b, int32_t variant);
 /* info = {members, tiles, tile elements, stages, graph replays, kernel launches} */
 int hlbm_batch_info(hlbm_batch* b, int64_t info[6]);
+/* the batch's cudaStream_t (every batched launch is issued on it), as a pointer-sized handle */
+void* hlbm_batch_stream(hlbm_batch* b);
 int hlbm_batch_destroy(hlbm_batch* b);
 
 /* simulation_state for callers that cannot allocate device memory, such as an analysis hook

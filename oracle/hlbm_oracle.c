@@ -66,6 +66,7 @@ typedef struct {
   double Fext[3], celerity, dtLB, nuth, nu, tau, avg_rho;
   int nobs;
   orc_obstacle* obs;
+  double* fs; /* streamed populations, for zero_gradient */
 } orc_lattice;
 
 static inline int64_t IDX(const orc_lattice* g, int x, int y, int z) {
@@ -186,6 +187,7 @@ void orc_destroy(void* h) {
     free(g->fi[p]);
   }
   free(g->obs);
+  free(g->fs);
   free(g);
 }
 
@@ -813,6 +815,33 @@ int32_t orc_lid_driven_cavity(void* h, int32_t face, const double Uphys[3]) {
   return 0;
 }
 
+/* ------------------------------------------------------- zero-gradient outlet */
+void orc_snapshot_streamed(void* h) {
+  orc_lattice* g = (orc_lattice*)h;
+  if (!g->fs) g->fs = (double*)malloc(sizeof(double) * Q * (size_t)g->ncell);
+  memcpy(g->fs, g->f, sizeof(double) * Q * (size_t)g->ncell);
+}
+
+int32_t orc_zero_gradient(void* h, int32_t face) {
+  orc_lattice* g = (orc_lattice*)h;
+  if (face < 0 || face > 5 || !g->fs) return -1;
+  const int axis = face / 2;
+  const int step = (face & 1) ? -1 : 1; /* towards the interior */
+  const int64_t nc = g->ncell, n = g->nplane[face];
+  int64_t shift = 1;
+  for (int d = 0; d < axis; d++) shift *= g->L[d];
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t idx = g->plane[face][i];
+    if (g->obst[idx] != FLUID) continue; /* like the neumann / lid operators: fluid nodes only */
+    const int64_t nb = idx + step * shift;
+    for (int k = 0; k < 5; k++) {
+      const int c = POST_IDS[face][k];
+      g->f[c * nc + idx] = g->fs[c * nc + nb];
+    }
+  }
+  return 0;
+}
+
 /* ------------------------------------------------------- simulation state */
 void orc_simulation_state(void* h, double out[3]) {
   orc_lattice* g = (orc_lattice*)h;
@@ -830,6 +859,60 @@ void orc_simulation_state(void* h, double out[3]) {
   out[0] = s;
   out[1] = vmin;
   out[2] = vmax;
+}
+
+/* init_double_couette (double_couette.hpp:25-49, init_double_couette.cu:74-100): f = feq(1, u)
+ * with u = Uc - dU * g over the Real box, g the global index along dim, Uc = U / c,
+ * dU = Uc / (0.5 * (n[dim] - 1)); the functor's operation order. */
+void orc_init_double_couette(void* h, const double U[3], int32_t dim) {
+  orc_lattice* g = (orc_lattice*)h;
+  const int64_t nc = g->ncell;
+  double uc[3], du[3];
+  for (int d = 0; d < 3; d++) uc[d] = U[d] / g->celerity;
+  for (int d = 0; d < 3; d++) du[d] = uc[d] / (0.5 * (g->n[dim] - 1));
+  for (int z = 2; z < g->L[2] - 2; z++)
+    for (int y = 2; y < g->L[1] - 2; y++)
+      for (int x = 2; x < g->L[0] - 2; x++) {
+        const int64_t idx = IDX(g, x, y, z);
+        const double v = (double)((dim == 0 ? x : (dim == 1 ? y : z)) - 2);
+        const double ux = uc[0] - du[0] * v, uy = uc[1] - du[1] * v, uz = uc[2] - du[2] * v;
+        const double u_squ = ux * ux + uy * uy + uz * uz;
+        for (int i = 0; i < Q; i++) {
+          const double eu = ux * EX[i] + uy * EY[i] + uz * EZ[i];
+          g->f[i * nc + idx] = 1. * W[i] * (1. + 3. * eu + 4.5 * eu * eu - 1.5 * u_squ);
+        }
+      }
+}
+
+/* plane_velocity_profile (plane_velocity_profile.cu:64-90, 179-260): per plane of the Real box
+ * normal to dim, sum / count / min / max of |dx / dtLB * u| over fluid nodes, from the current m1
+ * (call orc_macro_variables first for the current state).  avg = sum / count (0 when empty). */
+void orc_plane_velocity_profile(void* h, int32_t dim, double* avg, double* vmin, double* vmax, int64_t* count) {
+  orc_lattice* g = (orc_lattice*)h;
+  const int64_t nc = g->ncell;
+  const int n = g->n[dim];
+  const double ratio = g->dx / g->dtLB;
+  double* sum = (double*)calloc((size_t)n, sizeof(double));
+  for (int i = 0; i < n; i++) {
+    vmin[i] = 1.79769313486231570815e+308;
+    vmax[i] = -1.79769313486231570815e+308;
+    count[i] = 0;
+  }
+  for (int z = 2; z < g->L[2] - 2; z++)
+    for (int y = 2; y < g->L[1] - 2; y++)
+      for (int x = 2; x < g->L[0] - 2; x++) {
+        const int64_t idx = IDX(g, x, y, z);
+        if (g->obst[idx] != FLUID) continue;
+        const int out = (dim == 0 ? x : (dim == 1 ? y : z)) - 2;
+        const double ax = ratio * g->m1[idx], ay = ratio * g->m1[nc + idx], az = ratio * g->m1[2 * nc + idx];
+        const double v = sqrt(ax * ax + ay * ay + az * az);
+        sum[out] += v;
+        count[out] += 1;
+        if (vmin[out] > v) vmin[out] = v;
+        if (vmax[out] < v) vmax[out] = v;
+      }
+  for (int i = 0; i < n; i++) avg[i] = count[i] > 0 ? sum[i] / (double)count[i] : 0.0;
+  free(sum);
 }
 
 /* ---------------------------------------------------------------- access */

@@ -64,8 +64,18 @@ void orc_streaming(void* h);                            /* streaming.cu:68-118 (
 void orc_update_ghost(void* h);                         /* update_ghost.hpp:57-70, one rank */
 int32_t orc_neumann(void* h, int32_t face, const double U[3]);           /* neuman.cu:69-122 */
 int32_t orc_lid_driven_cavity(void* h, int32_t face, const double U[3]); /* lid_driven_cavity.cu:69-93 */
+/* zero_gradient outlet: an operator this project adds (no reference counterpart).  After
+ * orc_snapshot_streamed (called right after streaming), on the plane of `face` the populations
+ * entering from outside take the streamed values of the interior neighbour one node inside. */
+void orc_snapshot_streamed(void* h);
+int32_t orc_zero_gradient(void* h, int32_t face);
 /* simulation_state (simulation_state.cu:73-98): out = {sum rho, min |u|, max |u|} over Real */
 void orc_simulation_state(void* h, double out[3]);
+
+/* init_double_couette (init_double_couette.cu:74-100); dim 0 x, 1 y, 2 z */
+void orc_init_double_couette(void* h, const double U[3], int32_t dim);
+/* plane_velocity_profile (plane_velocity_profile.cu:64-90, 179-260) from the current m1 */
+void orc_plane_velocity_profile(void* h, int32_t dim, double* avg, double* vmin, double* vmax, int64_t* count);
 
 /* accessors: info = {L[3], n[3], ncell, plane sizes[6]} */
 void orc_info(void* h, int64_t info[13]);

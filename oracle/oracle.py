@@ -72,6 +72,10 @@ def _lib(kind: str):
         "orc_neumann": (C.c_int32, [vp, C.c_int32, d3]),
         "orc_lid_driven_cavity": (C.c_int32, [vp, C.c_int32, d3]),
         "orc_simulation_state": (None, [vp, d3]),
+        "orc_snapshot_streamed": (None, [vp]),
+        "orc_zero_gradient": (C.c_int32, [vp, C.c_int32]),
+        "orc_init_double_couette": (None, [vp, d3, C.c_int32]),
+        "orc_plane_velocity_profile": (None, [vp, C.c_int32, d3, d3, d3, C.POINTER(C.c_int64)]),
         "orc_info": (None, [vp, C.POINTER(C.c_int64)]),
         "orc_f": (d3, [vp]),
         "orc_m0": (d3, [vp]),
@@ -80,6 +84,8 @@ def _lib(kind: str):
         "orc_level": (i3, [vp]),
     }
     for name, (res, args) in sig.items():
+        if not hasattr(lib, name):  # operators the reference does not have
+            continue
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
@@ -158,6 +164,20 @@ class OracleLattice:
         self.lib.orc_simulation_state(self.h, out)
         return tuple(out)
 
+    def plane_velocity_profile(self, dimension: str = "Z"):
+        """(mean, min, max, count) per plane of the current state (macro_variables refreshed)."""
+        if not hasattr(self.lib, "orc_plane_velocity_profile"):
+            raise ValueError("plane_velocity_profile is restated by the C oracle only")
+        dim = {"X": 0, "Y": 1, "Z": 2}[dimension.upper()]
+        n = self.n[dim]
+        avg, vmin, vmax = np.empty(n), np.empty(n), np.empty(n)
+        cnt = np.empty(n, dtype=np.int64)
+        self.lib.orc_macro_variables(self.h)
+        dp = C.POINTER(C.c_double)
+        self.lib.orc_plane_velocity_profile(self.h, dim, avg.ctypes.data_as(dp), vmin.ctypes.data_as(dp),
+                                            vmax.ctypes.data_as(dp), cnt.ctypes.data_as(C.POINTER(C.c_int64)))
+        return avg, vmin, vmax, cnt
+
     # ----------------------------------------------------------- initialise
     def initialize(self):
         """config_initialize.msp:14-32 after domain/build_traversal/define_grid/init_obst."""
@@ -167,6 +187,8 @@ class OracleLattice:
                                c.tau if c.tau is not None else 0.0, c.dt)
         for value, bounds6 in c.init_distributions:
             lib.orc_set_distribution(self.h, value, _d(bounds6) if bounds6 else None, 0)
+        if getattr(c, "double_couette", None):
+            lib.orc_init_double_couette(self.h, _d(c.double_couette["U"]), "XYZ".index(c.double_couette["dimension"]))
         lib.orc_init_obstacles(self.h)
         for kind, oid, prm in c.obstacles:
             if kind == "ball":
@@ -196,6 +218,11 @@ class OracleLattice:
         elif op.name == "lid_driven_cavity":
             for r in s["regions"]:
                 lib.orc_lid_driven_cavity(h, _FACE_OF_PLANE[r], _d(s["U"]))
+        elif op.name == "zero_gradient":
+            if not hasattr(lib, "orc_zero_gradient"):
+                raise ValueError("zero_gradient has no reference counterpart")
+            for r in s["regions"]:
+                lib.orc_zero_gradient(h, _FACE_OF_PLANE[r])
         elif op.name == "set_distribution":
             b = s.get("bounds")
             b6 = None
@@ -220,6 +247,8 @@ class OracleLattice:
             for op in c.pre_stream_bcs:
                 self._op(op)
             self.lib.orc_streaming(self.h)
+            if any(op.name == "zero_gradient" for op in c.post_stream_bcs + c.boundary_conditions):
+                self.lib.orc_snapshot_streamed(self.h)
             for op in c.post_stream_bcs:
                 self._op(op)
             for op in c.boundary_conditions:

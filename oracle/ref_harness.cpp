@@ -43,6 +43,7 @@
 #include <hippoLBM/bcs/cavity.hpp>
 #include <hippoLBM/bcs/lid_driven_cavity.hpp>
 #include <hippoLBM/bcs/neumann.hpp>
+#include <hippoLBM/prepro/double_couette.hpp>
 // obstacles + io
 #include <hippoLBM/io/simulation_state.hpp>
 #include <hippoLBM/obstacle/obstacle.hpp>
@@ -457,6 +458,23 @@ int32_t orc_lid_driven_cavity(void* h, int32_t face, const double U[3]) {  // li
 #pragma omp parallel for schedule(static)
   for (size_t i = 0; i < t.size_; i++) bcs(t.ptr_[i]);
   return 0;
+}
+
+// init_double_couette (init_double_couette.cu:74-100): the reference functor over the Real box
+void orc_init_double_couette(void* h, const double U[3], int32_t dim) {
+  RefLattice* g = L(h);
+  const Vec3d Uc = Vec3d{U[0], U[1], U[2]} / g->P.celerity_;
+  FieldView<Q> pf = g->F.distributions();
+  Box3D real = g->G.build_box<Area::Local, Traversal::Real>();
+  auto run = [&](auto func) {
+    for (int z = real.start(2); z <= real.end(2); z++)
+      for (int y = real.start(1); y <= real.end(1); y++)
+        for (int x = real.start(0); x <= real.end(0); x++) func(onikaInt3_t{x, y, z});
+  };
+  const Vec3d dU = Uc / (0.5 * (g->n[dim] - 1));
+  if (dim == 0) run(InitDoubleCouetteFunc<Q, DIMX>{g->G, pf, dU, Uc});
+  if (dim == 1) run(InitDoubleCouetteFunc<Q, DIMY>{g->G, pf, dU, Uc});
+  if (dim == 2) run(InitDoubleCouetteFunc<Q, DIMZ>{g->G, pf, dU, Uc});
 }
 
 void orc_simulation_state(void* h, double out[3]) {  // simulation_state.cu:73-98, serial order

@@ -79,6 +79,20 @@ def builtin_cases():
                         Op("cavity_z_l", {"U": [0.03, 0.0, 0.0]}), Op("wall_bounce_back")],
         post_stream_bcs=[Op("post_bounce_back")],
         boundary_conditions=[Op("neumann", {"U": [0.0, 0.0, 0.0], "regions": ["plan_yz_l"]})], steps=80))
+    # init_double_couette (lbm_prepro_double_couette.msp shape): linear profile along Z / X, Zou/He
+    # planes moving in opposite directions
+    cases.append(Case(
+        name="double_couette_z_20x12x24", cell_dims=(19, 11, 23), bmin=(0, 0, 0), bmax=(0.19, 0.11, 0.23),
+        periodic=(True, True, False), nuth=1e-2, celerity=1.0, double_couette={"U": [0.001, 0.0, 0.0], "dimension": "Z"},
+        boundary_conditions=[Op("neumann", {"U": [-0.001, 0.0, 0.0], "regions": ["plan_xy_l"]}),
+                             Op("neumann", {"U": [0.001, 0.0, 0.0], "regions": ["plan_xy_0"]})],
+        steps=20))
+    cases.append(Case(
+        name="double_couette_x_18x10x8", cell_dims=(17, 9, 7), bmin=(0, 0, 0), bmax=(17, 9, 7),
+        periodic=(False, True, True), tau=0.8, nuth=0.1, double_couette={"U": [0.0, 0.02, 0.01], "dimension": "X"},
+        boundary_conditions=[Op("neumann", {"U": [0.0, -0.02, -0.01], "regions": ["plan_yz_l"]}),
+                             Op("neumann", {"U": [0.0, 0.02, 0.01], "regions": ["plan_yz_0"]})],
+        steps=15))
     return cases
 
 
@@ -110,6 +124,10 @@ def main():
     for path in sorted(glob.glob(os.path.join(args.reference, "regression-test", "*.msp"))):
         c = deck.load_msp(path)
         cases.append(c)
+    # the reference's double-Couette example deck (init_double_couette), parsed as a user deck
+    c = deck.load_msp(os.path.join(args.reference, "example", "lbm_prepro_double_couette.msp"))
+    c.name = "example_prepro_double_couette"
+    cases.append(c)
     cases += builtin_cases()
     out = {}
     for c in cases:

@@ -111,3 +111,36 @@ def test_batch_any_row_length_and_pipelined_rejects_unaligned():
         b.tune(6)
         with pytest.raises(capi.HlbmError):
             b.add(lat)
+
+
+@pytest.mark.parametrize("variant", [8, 6])
+def test_f16_members_equal_their_batch_of_one(variant):
+    """16-bit storage with stochastic rounding: the random bits hash each member's own node index
+    and step count, so a member's populations in the mixed batch equal those of the same lattice in
+    a batch of its own, bit for bit, whatever joins or leaves around it."""
+    from hippolbm_b200.batch import Batch
+    from hippolbm_b200.lattice import Lattice
+
+    lats = [Lattice.from_case(c, "f16") for c in CASES]
+    with Batch("f16") as b:
+        b.tune(variant)
+        for lat in lats[:3]:
+            b.add(lat)
+        b.step(5)
+        for lat in lats[3:]:
+            b.add(lat)     # join with 0 steps while the others are at 5
+        b.step(12)
+        out = [(lat.info()["steps"], lat.populations()) for lat in lats]
+        for lat in lats:
+            b.remove(lat)
+    for case, lat, (n, f) in zip(CASES, lats, out):
+        lat.close()
+        with Lattice.from_case(case, "f16") as one:
+            with Batch("f16") as b1:
+                b1.tune(variant)
+                b1.add(one)
+                b1.step(n)
+                b1.remove(one)
+            f1 = one.populations()
+            m = carried(case, one.flags())
+        assert np.array_equal(f[:, m], f1[:, m]), case.name
