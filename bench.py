@@ -65,9 +65,8 @@ def parse_args():
     ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="precision workload: linear scale of the 1024x256x256 channel (steps scale alike)")
-    ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,f16:shift,bf16",
-                    help="precision workload: storage tiers; options after ':' joined by '+': "
-                         "nearest (round-to-nearest storage), shift (deviations from feq at the inflow)")
+    ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,bf16",
+                    help="precision workload: storage tiers (\":nearest\": round-to-nearest storage)")
     ap.add_argument("--members", type=int, default=256, help="batch workload: lattices")
     ap.add_argument("--member-steps", type=int, default=2000, help="batch workload: steps of every lattice")
     ap.add_argument("--alone-steps", type=int, default=200,

@@ -33,7 +33,6 @@ SIGNATURES = {
     "hlbm_collision": (C.c_int, [_vp, C.c_int32, _d3]),
     "hlbm_storage_scale": (C.c_int, [_vp, C.c_double, C.c_double]),
     "hlbm_storage_rounding": (C.c_int, [_vp, C.c_int32]),
-    "hlbm_storage_reference": (C.c_int, [_vp, C.c_double, _d3]),
     "hlbm_set_distribution": (C.c_int, [_vp, C.c_double, _d3, C.c_int32]),
     "hlbm_init_double_couette": (C.c_int, [_vp, _d3, C.c_int32]),
     "hlbm_init_obstacles": (C.c_int, [_vp]),

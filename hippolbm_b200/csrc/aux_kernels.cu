@@ -529,6 +529,26 @@ cudaError_t launch_plane_profile(int prec, const void* f, const int8_t* flags, c
   return cudaGetLastError();
 }
 
+// 16-bit storage re-encoding: decode under the old storage parameters, encode under the new
+template <typename S, typename R>
+__global__ void k_reencode(S* __restrict__ f, const StepPlan po, const StepPlan pn) {
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < pn.ncell;
+       idx += (int64_t)gridDim.x * blockDim.x)
+    Unroll<0, Q>::run([&]<int I>() {
+      S* a = f + I * pn.stride + idx;
+      *a = Codec<S, R>::template enc<I>(Codec<S, R>::template dec<I>(*a, po), pn);
+    });
+}
+
+cudaError_t launch_reencode(int prec, void* f, const StepPlan& old_plan, const StepPlan& new_plan, cudaStream_t s) {
+  const int nb = stats_blocks(new_plan.ncell);
+  if (prec == 3)
+    k_reencode<__half, float><<<nb, 256, 0, s>>>(static_cast<__half*>(f), old_plan, new_plan);
+  else if (prec == 4)
+    k_reencode<__nv_bfloat16, float><<<nb, 256, 0, s>>>(static_cast<__nv_bfloat16*>(f), old_plan, new_plan);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s) {
   const int nb = stats_blocks(p.ncell);
   switch (prec) {

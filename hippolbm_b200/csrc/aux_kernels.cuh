@@ -34,6 +34,7 @@ cudaError_t launch_wall_force(int prec, const void* fpost, const int8_t* flags, 
                               double* out4, cudaStream_t s);
 cudaError_t launch_plane_profile(int prec, const void* f, const int8_t* flags, const StepPlan& p, int dim,
                                  double ratio, double* out4n, cudaStream_t s);
+cudaError_t launch_reencode(int prec, void* f, const StepPlan& old_plan, const StepPlan& new_plan, cudaStream_t s);
 cudaError_t launch_decode(int prec, const void* f, double* out, int dir, const StepPlan& p, cudaStream_t s);
 cudaError_t launch_encode(int prec, void* f, const double* in, int dir, const StepPlan& p, cudaStream_t s);
 

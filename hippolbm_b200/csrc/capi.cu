@@ -77,7 +77,7 @@ struct hlbm_ctx {
   double Fext[3], celerity, dtLB, nuth, nu, tau, avg_rho;
   int collision = 0;
   double mrt[8];
-  double rho0 = 1.0, scale = 1.0, u0[3] = {0.0, 0.0, 0.0};
+  double rho0 = 1.0, scale = 1.0;
   std::vector<HookOp> hooks;
   std::vector<ObstacleDesc> obstacles;
   void* f[2] = {nullptr, nullptr};
@@ -118,6 +118,32 @@ void mrt_reference(double r[8]) {  // mrt.hpp:43-47
   r[7] = 0;
 }
 
+// The 16-bit tiers store f_i - d_i with d_i the rest equilibrium of the lattice's collision at
+// density rho0: w_i * rho0 for BGK; for MRT the isotropic state with the MRT model's rest moments
+// (rho0, e = -11 rho0, eps = w_eps * rho0), which differs from w_i * rho0 unless w_eps = 3.  Stored
+// deviations then stay of the order of the flow's own perturbation, and so do the rounding steps.
+void storage_reference(const hlbm_ctx* c, float dref[Q]) {
+  double a = 1.0 / 3.0, b = 1.0 / 18.0, cc = 1.0 / 36.0;  // rest populations f0, f1..6, f7..18
+  if (c->collision == 1) {
+    // a + 6b + 12c = 1, -30a - 66b + 96c = -11, 12a - 24b + 12c = w_eps (Cramer's rule)
+    const double A[3][3] = {{1, 6, 12}, {-30, -66, 96}, {12, -24, 12}}, r[3] = {1, -11, c->mrt[5]};
+    auto det3 = [](const double M[3][3]) {
+      return M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+             M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    };
+    const double D = det3(A);
+    double x[3];
+    for (int k = 0; k < 3; k++) {
+      double B[3][3];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) B[i][j] = j == k ? r[i] : A[i][j];
+      x[k] = det3(B) / D;
+    }
+    a = x[0], b = x[1], cc = x[2];
+  }
+  for (int i = 0; i < Q; i++) dref[i] = float((i == 0 ? a : (i <= 6 ? b : cc)) * c->rho0);
+}
+
 void base_plan(hlbm_ctx* c, StepPlan& p) {
   std::memset(&p, 0, sizeof(p));
   p.nx = c->n[0];
@@ -129,11 +155,7 @@ void base_plan(hlbm_ctx* c, StepPlan& p) {
   p.rho0 = c->rho0;
   p.scale = c->scale;
   p.inv_scale = 1.0 / c->scale;
-  const double uu = c->u0[0] * c->u0[0] + c->u0[1] * c->u0[1] + c->u0[2] * c->u0[2];
-  for (int i = 0; i < Q; i++) {  // feq_i(rho0, u0); u0 = 0 gives w_i * rho0
-    const double eu = D3Q19::ex[i] * c->u0[0] + D3Q19::ey[i] * c->u0[1] + D3Q19::ez[i] * c->u0[2];
-    p.dref[i] = float(W_OF(i) * c->rho0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu));
-  }
+  storage_reference(c, p.dref);
   p.rounding = c->rounding;
   p.seed = uint32_t(c->steps);
 }
@@ -529,44 +551,44 @@ int hlbm_get_parameters(hlbm_ctx* c, double out[9]) {
   return HLBM_OK;
 }
 
+// Re-encode the carried state after the storage reference or scale changed (16-bit tiers): each
+// stored value is decoded under the old plan and encoded under the new one, on the device.
+static int reencode_storage(hlbm_ctx* c, const StepPlan& old_plan) {
+  if (c->precision != HLBM_F16 && c->precision != HLBM_BF16) return HLBM_OK;
+  if (c->phase == MATER) c->phase = POSTCOL;  // the read-out copy is recomputed when needed
+  StepPlan p;
+  base_plan(c, p);
+  bool same = p.scale == old_plan.scale;
+  for (int i = 0; i < Q; i++) same = same && p.dref[i] == old_plan.dref[i];
+  if (same) return HLBM_OK;
+  c->launches++;
+  HLBM_CK(launch_reencode(c->precision, c->f[c->cur], old_plan, p, c->stream));
+  return HLBM_OK;
+}
+
 int hlbm_collision(hlbm_ctx* c, int32_t kind, const double* rates8) {
   if (!c || (kind != 0 && kind != 1)) return fail(HLBM_EINVAL, "hlbm_collision: kind must be 0 (bgk) or 1 (mrt)");
+  if (int rc = set_device(c)) return rc;
+  StepPlan old_plan;
+  base_plan(c, old_plan);
   c->collision = kind;
   if (rates8)
     std::memcpy(c->mrt, rates8, sizeof(c->mrt));
   else
     mrt_reference(c->mrt);
   c->plan_dirty = true;
-  return HLBM_OK;
-}
-
-// re-encode the current state under new deviation parameters
-static int set_storage(hlbm_ctx* c, double rho0, double scale, const double u0[3]) {
-  int rc = make_raw(c);
-  if (rc) return rc;
-  std::vector<double> host;
-  if (c->precision == HLBM_F16 || c->precision == HLBM_BF16) {
-    host.resize(size_t(Q) * c->ncell);
-    if ((rc = hlbm_get_populations(c, host.data()))) return rc;
-  }
-  c->rho0 = rho0;
-  c->scale = scale;
-  for (int d = 0; d < 3; d++) c->u0[d] = u0[d];
-  c->plan_dirty = true;
-  if (!host.empty()) return hlbm_put_populations(c, host.data());
-  return HLBM_OK;
+  return reencode_storage(c, old_plan);  // the 16-bit storage reference follows the collision
 }
 
 int hlbm_storage_scale(hlbm_ctx* c, double rho0, double scale) {
   if (!c || !(scale > 0)) return fail(HLBM_EINVAL, "hlbm_storage_scale: scale must be > 0");
-  return set_storage(c, rho0, scale, c->u0);
-}
-
-int hlbm_storage_reference(hlbm_ctx* c, double rho0, const double u0[3]) {
-  if (!c || !u0) return fail(HLBM_EINVAL, "hlbm_storage_reference: NULL argument");
-  if (!(std::fabs(u0[0]) < 0.5 && std::fabs(u0[1]) < 0.5 && std::fabs(u0[2]) < 0.5))
-    return fail(HLBM_EINVAL, "hlbm_storage_reference: |u0| components must be below 0.5 (lattice units)");
-  return set_storage(c, rho0, c->scale, u0);
+  if (int rc = set_device(c)) return rc;
+  StepPlan old_plan;
+  base_plan(c, old_plan);
+  c->rho0 = rho0;
+  c->scale = scale;
+  c->plan_dirty = true;
+  return reencode_storage(c, old_plan);
 }
 
 int hlbm_storage_rounding(hlbm_ctx* c, int32_t mode) {
@@ -966,7 +988,7 @@ struct CheckpointHeader {
   int32_t n[3], periodic[3];
   int32_t phase, rounding;
   int64_t steps, ncell;
-  double rho0, scale, u0[3];
+  double rho0, scale;
 };
 constexpr char CKPT_MAGIC[8] = {'H', 'L', 'B', 'M', 'C', 'K', 'P', '1'};
 int64_t checkpoint_bytes(const hlbm_ctx* c) {
@@ -1000,7 +1022,6 @@ int hlbm_checkpoint_save(hlbm_ctx* c, void* host, int64_t bytes) {
   h.ncell = c->ncell;
   h.rho0 = c->rho0;
   h.scale = c->scale;
-  for (int d = 0; d < 3; d++) h.u0[d] = c->u0[d];
   unsigned char* out = static_cast<unsigned char*>(host);
   std::memcpy(out, &h, sizeof(h));
   out += sizeof(h);
@@ -1039,7 +1060,6 @@ int hlbm_checkpoint_load(hlbm_ctx* c, const void* host, int64_t bytes) {
   c->rounding = h.rounding;
   c->rho0 = h.rho0;  // the stored deviations are relative to these
   c->scale = h.scale;
-  for (int d = 0; d < 3; d++) c->u0[d] = h.u0[d];
   c->plan_dirty = true;
   return HLBM_OK;
 }

@@ -143,15 +143,30 @@ cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fo
 }
 
 // tile-list kernel of batches (variant 8: >= 3 CTAs per SM, 9: >= 2)
+template <typename S, typename R, bool STRICT, bool WALLS>
+cudaError_t launch_tiles_persistent(const TmaArgs& a, cudaStream_t s) {
+  auto kern = k_step_tiles_persistent<S, R, STRICT, WALLS, 3>;
+  static const int resident = [kern] {  // CTAs resident on the whole device
+    int per_sm = 0, dev = 0, sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (per_sm > 0 ? per_sm : 1) * sms;
+  }();
+  int grid = resident;
+  if (grid > a.ntiles) grid = a.ntiles;
+  if (grid < 1) return cudaSuccess;
+  kern<<<grid, 256, 0, s>>>(a.desc, a.tiles, a.ntiles, a.parity, a.seed, a.ndesc);
+  return cudaGetLastError();
+}
+
+// variant 8: persistent tile walk (3 CTAs of 256 threads per SM); 9: one CTA per tile
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_tiles(const TmaArgs& a, int walls, int variant, cudaStream_t s) {
-  if (variant == 9) {
-    if (walls) k_step_tiles<S, R, STRICT, true, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
-    else k_step_tiles<S, R, STRICT, false, 2><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
-  } else {
-    if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
-    else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
-  }
+  if (variant == 8)
+    return walls ? launch_tiles_persistent<S, R, STRICT, true>(a, s) : launch_tiles_persistent<S, R, STRICT, false>(a, s);
+  if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
+  else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
   return cudaGetLastError();
 }
 

@@ -50,41 +50,60 @@ struct Codec<float, float> {
   template <int I>
   __device__ static __forceinline__ float enc(float v, const StepPlan&) { return v; }
 };
+// 16-bit types store d_i * scale, d_i = f_i - dref_i (dref: the storage reference of the plan).
+// dec / enc convert full populations; decd / encd (and the stochastic encd_sr) convert the
+// deviations d_i themselves, which the step kernels carry for these tiers.
 template <>
 struct Codec<__half, float> {
+  template <int I>
+  __device__ static __forceinline__ float decd(__half s, const StepPlan& p) {
+    return __half2float(s) * (float)p.inv_scale;
+  }
+  template <int I>
+  __device__ static __forceinline__ __half encd(float d, const StepPlan& p) {
+    return __float2half_rn(d * (float)p.scale);
+  }
+  // stochastic rounding: the 13 FP32 mantissa bits below FP16's last bit get a random addend
+  // (the top 13 bits of r), then the value is truncated; Inf / NaN pass unchanged
+  template <int I>
+  __device__ static __forceinline__ __half encd_sr(float d, const StepPlan& p, uint32_t r) {
+    uint32_t b = __float_as_uint(d * (float)p.scale);
+    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 19;
+    return __float2half_rz(__uint_as_float(b));
+  }
   template <int I>
   __device__ static __forceinline__ float dec(__half s, const StepPlan& p) {
     return fmaf(__half2float(s), (float)p.inv_scale, p.dref[I]);
   }
   template <int I>
   __device__ static __forceinline__ __half enc(float v, const StepPlan& p) {
-    return __float2half_rn((v - p.dref[I]) * (float)p.scale);
-  }
-  // stochastic rounding: the 13 FP32 mantissa bits below FP16's last bit get a random addend
-  // (the top 13 bits of r), then the value is truncated; Inf / NaN pass unchanged
-  template <int I>
-  __device__ static __forceinline__ __half enc_sr(float v, const StepPlan& p, uint32_t r) {
-    uint32_t b = __float_as_uint((v - p.dref[I]) * (float)p.scale);
-    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 19;
-    return __float2half_rz(__uint_as_float(b));
+    return encd<I>(v - p.dref[I], p);
   }
 };
 template <>
 struct Codec<__nv_bfloat16, float> {
+  template <int I>
+  __device__ static __forceinline__ float decd(__nv_bfloat16 s, const StepPlan& p) {
+    return __bfloat162float(s) * (float)p.inv_scale;
+  }
+  template <int I>
+  __device__ static __forceinline__ __nv_bfloat16 encd(float d, const StepPlan& p) {
+    return __float2bfloat16_rn(d * (float)p.scale);
+  }
+  // stochastic rounding: a random addend to the 16 discarded bits, then truncation
+  template <int I>
+  __device__ static __forceinline__ __nv_bfloat16 encd_sr(float d, const StepPlan& p, uint32_t r) {
+    uint32_t b = __float_as_uint(d * (float)p.scale);
+    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 16;
+    return __ushort_as_bfloat16((unsigned short)(b >> 16));
+  }
   template <int I>
   __device__ static __forceinline__ float dec(__nv_bfloat16 s, const StepPlan& p) {
     return fmaf(__bfloat162float(s), (float)p.inv_scale, p.dref[I]);
   }
   template <int I>
   __device__ static __forceinline__ __nv_bfloat16 enc(float v, const StepPlan& p) {
-    return __float2bfloat16_rn((v - p.dref[I]) * (float)p.scale);
-  }
-  // stochastic rounding: a random addend to the 16 discarded bits, then truncation
-  template <int I>
-  __device__ static __forceinline__ __nv_bfloat16 enc_sr(float v, const StepPlan& p, uint32_t r) {
-    uint32_t b = __float_as_uint((v - p.dref[I]) * (float)p.scale);
-    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 16;
-    return __ushort_as_bfloat16((unsigned short)(b >> 16));
+    return encd<I>(v - p.dref[I], p);
   }
 };
 
@@ -136,20 +155,33 @@ struct Unroll<N, N> {
   __device__ static __forceinline__ void run(F&&) {}
 };
 
-// Stores the node's Q values to dst(I): stochastically rounded when the 16-bit tiers store the
-// carried state (MODE_PROLOGUE / MODE_FUSED with p.rounding), else rounded to nearest.  The
-// branch is taken once per node: selecting per value would make the compiler evaluate both
-// conversions for every value.
+// Stores the node's Q values to dst(I).  FP64 / FP32 tiers carry full populations; the 16-bit
+// tiers carry deviations from the storage reference, rounded stochastically when the state is
+// carried (MODE_PROLOGUE / MODE_FUSED with p.rounding), else to nearest.  The branch is taken
+// once per node: selecting per value would make the compiler evaluate both conversions.
 template <typename S, typename R, int MODE, class Dst>
 __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, int64_t idx, Dst&& dst) {
-  if constexpr (is_16bit<S>() && MODE != MODE_FINISH) {
-    if (p.rounding) {
+  if constexpr (is_16bit<S>()) {
+    if (MODE != MODE_FINISH && p.rounding) {
       const uint32_t h = node_hash(idx, p.seed);
-      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc_sr<I>(v[I], p, dir_bits<I>(h))); });
-      return;
+      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd_sr<I>(v[I], p, dir_bits<I>(h))); });
+    } else {
+      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd<I>(v[I], p)); });
     }
+  } else {
+    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc<I>(v[I], p)); });
   }
-  Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc<I>(v[I], p)); });
+}
+
+// A stored population as the step kernels carry it: the full value, or for the 16-bit tiers
+// its deviation from the storage reference.  dref is symmetric (dref_i = dref_opp(i)), so an
+// on-node bounce-back reads the opposite slot with the same meaning.
+template <typename S, typename R, int I>
+__device__ __forceinline__ R load_value(S raw, const StepPlan& p) {
+  if constexpr (is_16bit<S>())
+    return Codec<S, R>::template decd<I>(raw, p);
+  else
+    return Codec<S, R>::template dec<I>(raw, p);
 }
 
 template <typename R, int I>
@@ -287,7 +319,11 @@ __device__ __forceinline__ constexpr int mrt_den(int k) {
                           : (k == 9 ? (I >= 15 ? 18 : 36) : (k == 10 ? (I >= 15 ? 36 : 72) : MrtTables::BD_DIAG[k])));
 }
 
-template <typename R, bool STRICT>
+// DEVF: v holds deviations from the storage reference (the MRT rest state, whose moments are
+// rho0, e = -11 rho0, eps = w_eps rho0 and zero otherwise).  The moments of v are then the
+// deviations of the moments, the e / eps equilibria take the density deviation m[0], and only the
+// force term needs the full density rho0 + m[0].
+template <typename R, bool STRICT, bool DEVF = false>
 __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
   R m[19];
   Unroll<0, 19>::run([&]<int K>() {
@@ -358,7 +394,7 @@ __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
         first = false;
       }
     });
-    if (force) acc = acc + R(3.) * rho * weight<R, I>() * edot<I, R>(Fx, Fy, Fz);
+    if (force) acc = acc + R(3.) * (DEVF ? R(p.rho0) + rho : rho) * weight<R, I>() * edot<I, R>(Fx, Fy, Fz);
     v[I] = acc;
   });
 }
@@ -554,6 +590,73 @@ __device__ __forceinline__ void collide(R (&v)[Q], const StepPlan& p) {
     mrt<R, STRICT>(v, p);
 }
 
+// BGK on deviations d_i = f_i - w_i rho0 (the BGK storage reference): rho = rho0 + sum d,
+// j = sum e d, feq_i - w_i rho0 = w_i (rho - rho0) + w_i rho (3 e.u + 4.5 (e.u)^2 - 1.5 u^2).
+// Every sum runs over small numbers, so FP32 keeps the deviations' own precision and its rounding
+// does not accumulate into the mass the way a sum of full populations does.
+template <typename R>
+__device__ __forceinline__ void bgk_dev(R (&v)[Q], const StepPlan& p) {
+  R drho = v[0];
+#pragma unroll
+  for (int i = 1; i < Q; i++) drho = drho + v[i];
+  R ux = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
+  R uy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
+  R uz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
+  const R rho = R(p.rho0) + drho;
+  const R inv = R(1) / rho;
+  ux *= inv;
+  uy *= inv;
+  uz *= inv;
+  const R u_squ = (ux * ux + uy * uy + uz * uz);
+  const R inv_tau = R(p.inv_tau);
+  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  const bool force = p.has_force != 0;
+  Unroll<0, Q>::run([&]<int I>() {
+    constexpr R w = weight<R, I>();
+    const R eu = edot<I, R>(ux, uy, uz);
+    const R feqd = w * drho + w * rho * (R(3.) * eu + R(4.5) * eu * eu - R(1.5) * u_squ);
+    R d = (feqd - v[I]) * inv_tau;
+    if (force) d += R(3.) * rho * w * edot<I, R>(Fx, Fy, Fz);
+    v[I] += d;
+  });
+}
+
+template <typename R, int COLL>
+__device__ __forceinline__ void collide_dev(R (&v)[Q], const StepPlan& p) {
+  if (COLL == 0 || (COLL == 2 && p.collision == 0))
+    bgk_dev<R>(v, p);
+  else
+    mrt<R, false, true>(v, p);
+}
+
+// Everything after the gather: boundary operators on the nodes whose values were pulled
+// (`pulled` false for a first step, which collides the initial state), start_iteration boxes,
+// collision.  The 16-bit tiers carry deviations; the boundary operators and the boxes work on
+// full populations, so those nodes convert around them.
+template <typename S, typename R, bool STRICT, int MODE, int COLL>
+__device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin, int64_t idx, int x, int y, int z,
+                                            int8_t flag, const StepPlan& p, bool pulled, bool edge) {
+  constexpr bool DEV = is_16bit<S>();
+  if (pulled && edge && p.nops > 0) {
+    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] += R(p.dref[I]); });
+    plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
+    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] -= R(p.dref[I]); });
+  }
+  if (MODE != MODE_FINISH) {
+    for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
+      const SetBox& b = p.sets[s];
+      if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
+        Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>() - (DEV ? R(p.dref[I]) : R(0)); });
+    }
+    if (flag == FLAG_FLUID) {
+      if constexpr (DEV)
+        collide_dev<R, COLL>(v, p);
+      else
+        collide<R, STRICT, COLL>(v, p);
+    }
+  }
+}
+
 // The whole step for the node (x, y, z): gather (pull with periodic wrap and on-node
 // bounce-back), boundary operators, start_iteration boxes, collision, store.
 template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL>
@@ -568,7 +671,7 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
   }
   R v[Q];
   if (MODE == MODE_PROLOGUE) {
-    Unroll<0, Q>::run([&]<int I>() { v[I] = Codec<S, R>::template dec<I>(ld_stream(fin + I * p.stride + idx), p); });
+    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(ld_stream(fin + I * p.stride + idx), p); });
   } else {
     // source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others flag "outside"
     int sx[3], sy[3], sz[3];
@@ -599,19 +702,11 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
       if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
       const S* ptr = bounce ? fin + O * p.stride + idx : fin + I * p.stride + src;
       const S raw = ld_stream(ptr);
-      v[I] = bounce ? Codec<S, R>::template dec<O>(raw, p) : Codec<S, R>::template dec<I>(raw, p);
+      v[I] = bounce ? load_value<S, R, O>(raw, p) : load_value<S, R, I>(raw, p);
     });
-    const bool boundary = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
-    if (boundary && p.nops > 0) plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
   }
-  if (MODE != MODE_FINISH) {
-    for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
-      const SetBox& b = p.sets[s];
-      if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
-        Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
-    }
-    if (flag == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
-  }
+  const bool edge = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
+  node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, edge);
   store_node<S, R, MODE>(v, p, idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
 }
 

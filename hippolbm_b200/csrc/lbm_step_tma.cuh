@@ -247,11 +247,11 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
         constexpr int O = D3Q19::opp(I);
         const S* row = stage + size_t(I) * tile_elems + size_t(r) * nx;
         if (first) {  // own node, plane I
-          v[I] = Codec<S, R>::template dec<I>(row[x], p);
+          v[I] = load_value<S, R, I>(row[x], p);
           return;
         }
         if (I != 0 && row_bounces(p, y, z, ey, ez)) {  // the stage row holds this node's plane opp(I)
-          v[I] = Codec<S, R>::template dec<O>(row[x], p);
+          v[I] = load_value<S, R, O>(row[x], p);
           return;
         }
         int xs = x - ex;
@@ -266,18 +266,12 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
           bounce = L.flags[(int64_t(sz) * ny + sy) * nx + xs] == FLAG_WALL;
         }
         if (bounce)
-          v[I] = Codec<S, R>::template dec<O>(ld_stream(fin + O * stride + idx), p);
+          v[I] = load_value<S, R, O>(ld_stream(fin + O * stride + idx), p);
         else
-          v[I] = Codec<S, R>::template dec<I>(row[xs], p);
+          v[I] = load_value<S, R, I>(row[xs], p);
       });
-      if (!first && p.nops > 0 && (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1))
-        plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
-      for (int sb = 0; sb < p.nsets; sb++) {
-        const SetBox& b = p.sets[sb];
-        if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
-          Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
-      }
-      if (flag == FLAG_FLUID) collide<R, STRICT, 2>(v, p);
+      node_update<S, R, STRICT, MODE_FUSED, 2>(v, fin, idx, x, y, z, flag, p, !first,
+                                               x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1);
       store_node<S, R, MODE_FUSED>(v, p, idx, [&]<int I>(S s) { fout[I * stride + idx] = s; });
     }
     __syncwarp();

@@ -265,17 +265,9 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
   Unroll<0, NPT>::run([&]<int K>() {
     const int x = x0 + K;
     R v[Q];
-    Unroll<0, Q>::run([&]<int I>() { v[I] = Codec<S, R>::template dec<I>(c[I].template get<K>(), p); });
-    if (MODE != MODE_PROLOGUE && p.nops > 0 && (yz_face || x == 0 || x == p.nx - 1))
-      plane_ops<S, R>(v, fin, row + x, x, yy, z, fl[K], p);
-    if (MODE != MODE_FINISH) {
-      for (int s = 0; s < p.nsets; s++) {
-        const SetBox& b = p.sets[s];
-        if (x >= b.lo[0] && x <= b.hi[0] && yy >= b.lo[1] && yy <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
-          Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>(); });
-      }
-      if (fl[K] == FLAG_FLUID) collide<R, STRICT, COLL>(v, p);
-    }
+    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(c[I].template get<K>(), p); });
+    node_update<S, R, STRICT, MODE, COLL>(v, fin, row + x, x, yy, z, fl[K], p, MODE != MODE_PROLOGUE,
+                                          yz_face || x == 0 || x == p.nx - 1);
     store_node<S, R, MODE>(v, p, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
   });
   Unroll<0, Q>::run([&]<int I>() { c[I].store(fout + I * p.stride + row + x0); });

@@ -219,12 +219,6 @@ class Lattice:
         capi.check(self.L.hlbm_storage_rounding(self.h, {"nearest": 0, "stochastic": 1}[mode]))
         return self
 
-    def storage_reference(self, rho0: float = 1.0, u0=(0.0, 0.0, 0.0)):
-        """16-bit tiers store f_i - feq_i(rho0, u0): a reference velocity near the flow's mean
-        velocity shrinks the stored deviations (and the rounding steps)."""
-        capi.check(self.L.hlbm_storage_reference(self.h, float(rho0), capi.dvec(u0)))
-        return self
-
     def tune(self, variant: int):
         capi.check(self.L.hlbm_tune(self.h, int(variant)))
         return self

@@ -9,9 +9,8 @@ the FP64 run it reports
     difference from the FP64 drag;
   - the run's throughput (MLUPS, wall clock around the synchronised steps).
 The tiers are the library's precisions: "f64", "f32" (FP32 storage and arithmetic), "f16" /
-"bf16" (FP32 arithmetic, 16-bit storage of f_i - w_i rho0, stochastic rounding); the suffix
-":nearest" selects round-to-nearest storage and ":shift" stores deviations from the equilibrium at
-the inflow velocity instead of at rest.
+"bf16" (FP32 arithmetic in deviation form, 16-bit storage of f_i minus the collision's rest
+equilibrium, stochastic rounding); the suffix ":nearest" selects round-to-nearest storage.
 """
 from __future__ import annotations
 
@@ -23,25 +22,14 @@ from .deck import Case
 from .lattice import Lattice
 
 
-def inflow_velocity(case: Case) -> tuple:
-    """Lattice velocity of the case's first non-zero Zou/He (`neumann`) boundary, else zero."""
-    for op in case.post_stream_bcs + case.boundary_conditions:
-        if op.name == "neumann" and any(float(u) != 0.0 for u in op.slots.get("U", [])):
-            return tuple(float(u) / case.celerity for u in op.slots["U"])
-    return (0.0, 0.0, 0.0)
-
-
 def run_tier(case: Case, tier: str, steps: int, chunk: int = 1000, device: int = 0, variant: int | None = None):
-    """Run `case` for `steps` at one tier -- a precision with options after ':' joined by '+':
-    "nearest" (round-to-nearest storage), "shift" (store deviations from feq(1, u_in), u_in the
-    inflow velocity) -- and return (u (3, nz, ny, nx) FP64, fluid mask, record)."""
+    """Run `case` for `steps` at one tier -- a precision, with ":nearest" for round-to-nearest
+    storage -- and return (u (3, nz, ny, nx) FP64, fluid mask, record)."""
     precision, _, opts = tier.partition(":")
     opts = [o for o in opts.split("+") if o]
     with Lattice.from_case(case, precision, device) as lat:
         if "nearest" in opts:
             lat.rounding("nearest")
-        if "shift" in opts:
-            lat.storage_reference(1.0, inflow_velocity(case))
         if variant is not None:
             lat.tune(variant)
         m0 = lat.moments()[0]

@@ -88,13 +88,12 @@ int hlbm_get_parameters(hlbm_ctx* ctx, double out[9]);
  * constants (mrt.hpp:43-47); s_nu = 1 / tau always. */
 int hlbm_collision(hlbm_ctx* ctx, int32_t kind, const double* rates8);
 
-/* Reduced-precision storage keeps (f_i - d_i) * scale with d_i = feq_i(rho0, u0), by default
- * w_i * rho0 (u0 = 0, rho0 = 1; HLBM_F16: scale 1024, HLBM_BF16: 1).  hlbm_storage_reference sets
- * a reference velocity u0 (lattice units): for a flow dominated by a known mean velocity the stored
- * deviations, hence the rounding steps, shrink.  Both re-encode the current state.  No reference
- * counterpart: part of the precision tiers. */
+/* Reduced-precision storage keeps (f_i - d_i) * scale, d_i the rest equilibrium of the lattice's
+ * collision at density rho0 (BGK: w_i * rho0; MRT: the isotropic state with the model's rest
+ * moments), rho0 = 1 and scale 1024 (HLBM_F16) or 1 (HLBM_BF16) by default.  Changing rho0, the
+ * scale or the collision re-encodes the current state on the device.  The 16-bit tiers collide in
+ * deviation form (f_i - d_i) in FP32.  No reference counterpart: part of the precision tiers. */
 int hlbm_storage_scale(hlbm_ctx* ctx, double rho0, double scale);
-int hlbm_storage_reference(hlbm_ctx* ctx, double rho0, const double u0[3]);
 /* Rounding of the 16-bit storage tiers when a step stores the state: 1 (the default) stochastic
  * -- round up with probability equal to the discarded fraction, from a hash of (node, step
  * number, direction), so results are reproducible and the same alone or in a batch -- or 0 round
@@ -211,8 +210,9 @@ void* hlbm_stream(hlbm_ctx* ctx);
  * made with hlbm_domain on the same device and precision, each with its own size, plan, collision
  * and boundary operators -- with ONE launch of the pipelined persistent kernel per time step, over
  * the concatenated tile list of all members; steps are replayed from a captured CUDA graph of two
- * steps.  Kernel (hlbm_batch_tune): 8 (default) / 9 = one CTA per tile of about 256 nodes with
- * direct pulls (at least 3 / 2 CTAs per SM), any lattice shape; 6 / 7 = the pipelined kernel
+ * steps.  Kernel (hlbm_batch_tune): tiles of about 256 nodes with direct pulls, any lattice
+ * shape -- 8 (default) a persistent grid of resident CTAs each walking a contiguous range of tiles,
+ * 9 one CTA per tile; 6 / 7 = the pipelined kernel
  * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0).  A
  * member that has not stepped yet takes its first step inside the batched launch.  While a
  * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.  A lattice
