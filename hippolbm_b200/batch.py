@@ -30,7 +30,7 @@ class Batch:
         return self
 
     def tune(self, variant: int):
-        """8: persistent tile walk (default); 9: one CTA per tile; 6 / 7: pipelined kernel."""
+        """8: one CTA per tile (default); 9: persistent tile walk; 6 / 7: pipelined kernel."""
         capi.check(self.L.hlbm_batch_tune(self.h, int(variant)))
         return self
 

@@ -27,6 +27,7 @@ SIGNATURES = {
     "hlbm_version": (C.c_char_p, []),
     "hlbm_domain": (C.c_int, [_i3, _d3, _d3, _i3, C.c_int32, C.c_int32, C.POINTER(_vp)]),
     "hlbm_destroy": (C.c_int, [_vp]),
+    "hlbm_trim_memory": (C.c_int, [C.c_int32]),
     "hlbm_lbm_parameters": (C.c_int, [_vp, _d3, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_double,
                                       C.c_double]),
     "hlbm_get_parameters": (C.c_int, [_vp, _d3]),

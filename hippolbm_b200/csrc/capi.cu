@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -60,6 +61,45 @@ size_t elem_size(int prec) {
 }
 
 constexpr double W_OF(int i) { return 1.0 / D3Q19::wden[i]; }
+
+// Device memory of lattices and batches comes from one stream-ordered pool per device that keeps
+// freed blocks for reuse (release threshold: unlimited).  Creating and destroying lattices while
+// others are stepping then costs no device-wide synchronisation: cudaFree waits for every stream
+// of the device, and in a solve server that can stall each retirement for hundreds of
+// milliseconds.  hlbm_trim_memory hands the cached blocks back to the driver.
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t device_pool(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (cudaMemPoolCreate(&g_pools[dev], &props) != cudaSuccess) {
+      cudaGetLastError();
+      g_pools[dev] = nullptr;
+      return nullptr;
+    }
+    uint64_t keep = ~uint64_t(0);
+    cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  return g_pools[dev];
+}
+
+// allocation in stream order on s (usable by work queued on s after it, or by other streams once
+// s has been synchronised); freed with pool_free on a stream whose earlier work used it last
+cudaError_t pool_alloc(void** ptr, size_t bytes, int dev, cudaStream_t s) {
+  cudaMemPool_t pool = device_pool(dev);
+  if (!pool) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(ptr, bytes, pool, s);
+}
+
+void pool_free(void* ptr, cudaStream_t s) {
+  if (ptr) cudaFreeAsync(ptr, s);
+}
 }  // namespace
 
 namespace hlbm {
@@ -196,8 +236,8 @@ bool pipeline_geometry(int nx, int ny, size_t es, int& rows, int& stages1, int& 
 int setup_pipeline(hlbm_ctx* c) {
   const StepPlan& p = c->plan;
   if (!c->plan_dev) {
-    if (cudaMalloc(&c->plan_dev, sizeof(StepPlan)) != cudaSuccess ||
-        cudaMalloc(&c->desc_dev, sizeof(LatticeDesc)) != cudaSuccess)
+    if (pool_alloc((void**)&c->plan_dev, sizeof(StepPlan), c->device, c->stream) != cudaSuccess ||
+        pool_alloc((void**)&c->desc_dev, sizeof(LatticeDesc), c->device, c->stream) != cudaSuccess)
       return fail(HLBM_ENOMEM, "cannot allocate the step plan");
   }
   HLBM_CK(cudaMemcpyAsync(c->plan_dev, &p, sizeof(StepPlan), cudaMemcpyHostToDevice, c->stream));
@@ -219,9 +259,9 @@ int setup_pipeline(hlbm_ctx* c) {
   for (int z = 0; z < p.nz; z++)
     for (int y0 = 0; y0 < p.ny; y0 += rows) tiles.push_back(make_int4(0, z, y0, (p.ny - y0) < rows ? (p.ny - y0) : rows));
   if (int(tiles.size()) != c->ntiles) {
-    cudaFree(c->tiles_dev);
+    pool_free(c->tiles_dev, c->stream);
     c->tiles_dev = nullptr;
-    if (cudaMalloc(&c->tiles_dev, tiles.size() * sizeof(Tile)) != cudaSuccess)
+    if (pool_alloc((void**)&c->tiles_dev, tiles.size() * sizeof(Tile), c->device, c->stream) != cudaSuccess)
       return fail(HLBM_ENOMEM, "cannot allocate the tile list");
   }
   HLBM_CK(cudaMemcpyAsync(c->tiles_dev, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
@@ -458,19 +498,20 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
     return cleanup(fail(HLBM_ECUDA, "cudaStreamCreate failed"));
   const size_t fbytes = size_t(Q) * c->stride * elem_size(precision);
   for (int k = 0; k < 2; k++)
-    if (cudaMalloc(&c->f[k], fbytes) != cudaSuccess) {
+    if (pool_alloc(&c->f[k], fbytes, c->device, c->stream) != cudaSuccess) {
       cudaGetLastError();
       return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate " + std::to_string(fbytes >> 20) +
                                            " MiB of populations"));
     }
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-  if (cudaMalloc(&c->err_dev, sizeof(int)) != cudaSuccess || cudaMemsetAsync(c->err_dev, 0, sizeof(int), c->stream) != cudaSuccess) {
+  if (pool_alloc((void**)&c->err_dev, sizeof(int), c->device, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->err_dev, 0, sizeof(int), c->stream) != cudaSuccess) {
     cudaGetLastError();
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate the error word"));
   }
-  if (cudaMalloc(&c->flags, size_t(c->ncell)) != cudaSuccess ||
-      cudaMalloc(&c->partials, sizeof(double) * 4 * 148 * 8) != cudaSuccess ||
-      cudaMalloc(&c->stats_dev, sizeof(double) * 4) != cudaSuccess) {
+  if (pool_alloc((void**)&c->flags, size_t(c->ncell), c->device, c->stream) != cudaSuccess ||
+      pool_alloc((void**)&c->partials, sizeof(double) * 4 * 148 * 8, c->device, c->stream) != cudaSuccess ||
+      pool_alloc((void**)&c->stats_dev, sizeof(double) * 4, c->device, c->stream) != cudaSuccess) {
     cudaGetLastError();
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate flags"));
   }
@@ -490,19 +531,12 @@ int hlbm_destroy(hlbm_ctx* c) {
   if (!c) return HLBM_OK;
   if (c->batch) hlbm_batch_remove(c->batch, c);  // a batch never keeps a destroyed member
   cudaSetDevice(c->device);
-  if (c->stream) cudaStreamSynchronize(c->stream);
-  cudaFree(c->f[0]);
-  cudaFree(c->f[1]);
-  cudaFree(c->flags);
-  cudaFree(c->partials);
-  cudaFree(c->stats_dev);
-  cudaFree(c->plane_tmp);
-  cudaFree(c->uprev);
-  cudaFree(c->plan_dev);
-  cudaFree(c->desc_dev);
-  cudaFree(c->tiles_dev);
-  cudaFree(c->err_dev);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream) {  // the memory returns to the pool once the stream's work is done
+    void* bufs[] = {c->f[0], c->f[1], c->flags, c->partials, c->stats_dev, c->plane_tmp, c->uprev,
+                    c->plan_dev, c->desc_dev, c->tiles_dev, c->err_dev};
+    for (void* b : bufs) pool_free(b, c->stream);
+    cudaStreamDestroy(c->stream);
+  }
   delete c;
   return HLBM_OK;
 }
@@ -803,9 +837,10 @@ int hlbm_macro_variables(hlbm_ctx* c, double* rho, double* u) {
   if (int rc = state_buffer(c, &s)) return rc;
   double *drho = nullptr, *du = nullptr;
   const size_t n = size_t(c->ncell);
-  if (rho && cudaMalloc(&drho, n * 8) != cudaSuccess) return fail(HLBM_ENOMEM, "hlbm_macro_variables: no memory");
-  if (u && cudaMalloc(&du, 3 * n * 8) != cudaSuccess) {
-    cudaFree(drho);
+  if (rho && pool_alloc((void**)&drho, n * 8, c->device, c->stream) != cudaSuccess)
+    return fail(HLBM_ENOMEM, "hlbm_macro_variables: no memory");
+  if (u && pool_alloc((void**)&du, 3 * n * 8, c->device, c->stream) != cudaSuccess) {
+    pool_free(drho, c->stream);
     return fail(HLBM_ENOMEM, "hlbm_macro_variables: no memory");
   }
   StepPlan p;
@@ -814,9 +849,9 @@ int hlbm_macro_variables(hlbm_ctx* c, double* rho, double* u) {
   cudaError_t e = launch_macro_stats(c->precision, s, c->flags, p, drho, du, c->partials, c->stats_dev, c->stream);
   if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, drho, n * 8, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && u) e = cudaMemcpyAsync(u, du, 3 * n * 8, cudaMemcpyDeviceToHost, c->stream);
+  pool_free(drho, c->stream);
+  pool_free(du, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(drho);
-  cudaFree(du);
   if (e != cudaSuccess) return fail(HLBM_ECUDA, std::string("hlbm_macro_variables: ") + cudaGetErrorString(e));
   return HLBM_OK;
 }
@@ -842,7 +877,7 @@ int hlbm_residual(hlbm_ctx* c, double* out) {
   if (int rc = state_buffer(c, &s)) return rc;
   int first = 0;
   if (!c->uprev) {
-    if (cudaMalloc(&c->uprev, size_t(c->ncell) * 3 * sizeof(float)) != cudaSuccess)
+    if (pool_alloc((void**)&c->uprev, size_t(c->ncell) * 3 * sizeof(float), c->device, c->stream) != cudaSuccess)
       return fail(HLBM_ENOMEM, "hlbm_residual: no memory for the velocity snapshot");
     first = 1;
   }
@@ -898,7 +933,7 @@ int hlbm_get_populations(hlbm_ctx* c, double* out) {
   if (elem_size(c->precision) == 8) {
     HLBM_CK(cudaMemcpy2DAsync(out, n * 8, s, size_t(c->stride) * 8, n * 8, Q, cudaMemcpyDeviceToHost, c->stream));
   } else {
-    if (!c->plane_tmp && cudaMalloc(&c->plane_tmp, n * 8) != cudaSuccess)
+    if (!c->plane_tmp && pool_alloc((void**)&c->plane_tmp, n * 8, c->device, c->stream) != cudaSuccess)
       return fail(HLBM_ENOMEM, "hlbm_get_populations: no memory");
     StepPlan p;
     base_plan(c, p);
@@ -921,7 +956,7 @@ int hlbm_put_populations(hlbm_ctx* c, const double* in) {
     HLBM_CK(cudaMemcpy2DAsync(c->f[c->cur], size_t(c->stride) * 8, in, n * 8, n * 8, Q, cudaMemcpyHostToDevice,
                               c->stream));
   } else {
-    if (!c->plane_tmp && cudaMalloc(&c->plane_tmp, n * 8) != cudaSuccess)
+    if (!c->plane_tmp && pool_alloc((void**)&c->plane_tmp, n * 8, c->device, c->stream) != cudaSuccess)
       return fail(HLBM_ENOMEM, "hlbm_put_populations: no memory");
     StepPlan p;
     base_plan(c, p);
@@ -958,7 +993,7 @@ int hlbm_plane_velocity_profile(hlbm_ctx* c, int32_t dim, double* avg, double* v
   if (int rc = state_buffer(c, &s)) return rc;
   const int n = c->n[dim];
   double* dev = nullptr;
-  if (cudaMalloc(&dev, size_t(4) * n * sizeof(double)) != cudaSuccess)
+  if (pool_alloc((void**)&dev, size_t(4) * n * sizeof(double), c->device, c->stream) != cudaSuccess)
     return fail(HLBM_ENOMEM, "hlbm_plane_velocity_profile: no memory");
   std::vector<double> host(size_t(4) * n);
   StepPlan p;
@@ -967,8 +1002,8 @@ int hlbm_plane_velocity_profile(hlbm_ctx* c, int32_t dim, double* avg, double* v
   cudaError_t e = launch_plane_profile(c->precision, s, c->flags, p, dim, c->dx / c->dtLB, dev, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host.data(), dev, host.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  pool_free(dev, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(dev);
   if (e != cudaSuccess) return fail(HLBM_ECUDA, std::string("hlbm_plane_velocity_profile: ") + cudaGetErrorString(e));
   for (int i = 0; i < n; i++) {
     const double sum = host[4 * i], cnt = host[4 * i + 1];
@@ -1198,15 +1233,15 @@ int batch_rebuild(hlbm_batch* b) {
     return batch_fail(HLBM_EPLAN, "batch tiles do not fit two pipeline stages");
   b->stages2 = stages2;
   if (b->members.size() > b->desc_cap) {
-    cudaFree(b->desc_dev);
+    pool_free(b->desc_dev, b->stream);
     b->desc_cap = std::max<size_t>(b->members.size(), 2 * b->desc_cap);
-    if (cudaMalloc(&b->desc_dev, b->desc_cap * sizeof(LatticeDesc)) != cudaSuccess)
+    if (pool_alloc((void**)&b->desc_dev, b->desc_cap * sizeof(LatticeDesc), b->device, b->stream) != cudaSuccess)
       return batch_fail(HLBM_ENOMEM, "batch descriptors");
   }
   if (tiles.size() > b->tiles_cap) {
-    cudaFree(b->tiles_dev);
+    pool_free(b->tiles_dev, b->stream);
     b->tiles_cap = std::max<size_t>(tiles.size(), 2 * b->tiles_cap);
-    if (cudaMalloc(&b->tiles_dev, b->tiles_cap * sizeof(Tile)) != cudaSuccess)
+    if (pool_alloc((void**)&b->tiles_dev, b->tiles_cap * sizeof(Tile), b->device, b->stream) != cudaSuccess)
       return batch_fail(HLBM_ENOMEM, "batch tile list");
   }
   if (!tiles.empty())
@@ -1289,7 +1324,9 @@ int hlbm_batch_create(int32_t precision, int32_t device, hlbm_batch** out) {
   b->device = device;
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&b->err_dev, sizeof(int)) != cudaSuccess || cudaMemset(b->err_dev, 0, sizeof(int)) != cudaSuccess) {
+      pool_alloc((void**)&b->err_dev, sizeof(int), device, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->err_dev, 0, sizeof(int), b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess) {
     cudaGetLastError();
     hlbm_batch_destroy(b);
     return fail(HLBM_ECUDA, "hlbm_batch_create: cannot set up the device");
@@ -1417,16 +1454,32 @@ int hlbm_batch_info(hlbm_batch* b, int64_t info[6]) {
 
 void* hlbm_batch_stream(hlbm_batch* b) { return b ? (void*)b->stream : nullptr; }
 
+int hlbm_trim_memory(int32_t device) {
+  if (device < 0 || device >= 64) return fail(HLBM_EINVAL, "hlbm_trim_memory: bad device");
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    pool = g_pools[device];
+  }
+  if (!pool) return HLBM_OK;
+  HLBM_CK(cudaSetDevice(device));
+  HLBM_CK(cudaDeviceSynchronize());
+  HLBM_CK(cudaMemPoolTrimTo(pool, 0));
+  return HLBM_OK;
+}
+
 int hlbm_batch_destroy(hlbm_batch* b) {
   if (!b) return HLBM_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (hlbm_ctx* c : b->members) c->batch = nullptr;
   batch_drop_graph(b);
-  cudaFree(b->desc_dev);
-  cudaFree(b->tiles_dev);
-  cudaFree(b->err_dev);
-  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->stream) {
+    pool_free(b->desc_dev, b->stream);
+    pool_free(b->tiles_dev, b->stream);
+    pool_free(b->err_dev, b->stream);
+    cudaStreamDestroy(b->stream);
+  }
   delete b;
   return HLBM_OK;
 }

@@ -160,10 +160,10 @@ cudaError_t launch_tiles_persistent(const TmaArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// variant 8: persistent tile walk (3 CTAs of 256 threads per SM); 9: one CTA per tile
+// variant 8: one CTA per tile; 9: persistent tile walk (3 CTAs of 256 threads per SM)
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_tiles(const TmaArgs& a, int walls, int variant, cudaStream_t s) {
-  if (variant == 8)
+  if (variant == 9)
     return walls ? launch_tiles_persistent<S, R, STRICT, true>(a, s) : launch_tiles_persistent<S, R, STRICT, false>(a, s);
   if (walls) k_step_tiles<S, R, STRICT, true, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);
   else k_step_tiles<S, R, STRICT, false, 3><<<a.ntiles, 256, 0, s>>>(a.desc, a.tiles, a.parity, a.seed, a.ndesc);

@@ -51,23 +51,23 @@ struct Codec<float, float> {
   __device__ static __forceinline__ float enc(float v, const StepPlan&) { return v; }
 };
 // 16-bit types store d_i * scale, d_i = f_i - dref_i (dref: the storage reference of the plan).
-// dec / enc convert full populations; decd / encd (and the stochastic encd_sr) convert the
-// deviations d_i themselves, which the step kernels carry for these tiers.
+// dec / enc convert full populations; decd / encd (and the stochastic encd_sr) convert the scaled
+// deviations d_i * scale themselves, which the step kernels carry for these tiers.
 template <>
 struct Codec<__half, float> {
   template <int I>
-  __device__ static __forceinline__ float decd(__half s, const StepPlan& p) {
-    return __half2float(s) * (float)p.inv_scale;
+  __device__ static __forceinline__ float decd(__half s, const StepPlan&) {
+    return __half2float(s);
   }
   template <int I>
-  __device__ static __forceinline__ __half encd(float d, const StepPlan& p) {
-    return __float2half_rn(d * (float)p.scale);
+  __device__ static __forceinline__ __half encd(float d, const StepPlan&) {
+    return __float2half_rn(d);
   }
   // stochastic rounding: the 13 FP32 mantissa bits below FP16's last bit get a random addend
   // (the top 13 bits of r), then the value is truncated; Inf / NaN pass unchanged
   template <int I>
-  __device__ static __forceinline__ __half encd_sr(float d, const StepPlan& p, uint32_t r) {
-    uint32_t b = __float_as_uint(d * (float)p.scale);
+  __device__ static __forceinline__ __half encd_sr(float d, const StepPlan&, uint32_t r) {
+    uint32_t b = __float_as_uint(d);
     if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 19;
     return __float2half_rz(__uint_as_float(b));
   }
@@ -77,23 +77,23 @@ struct Codec<__half, float> {
   }
   template <int I>
   __device__ static __forceinline__ __half enc(float v, const StepPlan& p) {
-    return encd<I>(v - p.dref[I], p);
+    return encd<I>((v - p.dref[I]) * (float)p.scale, p);
   }
 };
 template <>
 struct Codec<__nv_bfloat16, float> {
   template <int I>
-  __device__ static __forceinline__ float decd(__nv_bfloat16 s, const StepPlan& p) {
-    return __bfloat162float(s) * (float)p.inv_scale;
+  __device__ static __forceinline__ float decd(__nv_bfloat16 s, const StepPlan&) {
+    return __bfloat162float(s);
   }
   template <int I>
-  __device__ static __forceinline__ __nv_bfloat16 encd(float d, const StepPlan& p) {
-    return __float2bfloat16_rn(d * (float)p.scale);
+  __device__ static __forceinline__ __nv_bfloat16 encd(float d, const StepPlan&) {
+    return __float2bfloat16_rn(d);
   }
   // stochastic rounding: a random addend to the 16 discarded bits, then truncation
   template <int I>
-  __device__ static __forceinline__ __nv_bfloat16 encd_sr(float d, const StepPlan& p, uint32_t r) {
-    uint32_t b = __float_as_uint(d * (float)p.scale);
+  __device__ static __forceinline__ __nv_bfloat16 encd_sr(float d, const StepPlan&, uint32_t r) {
+    uint32_t b = __float_as_uint(d);
     if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 16;
     return __ushort_as_bfloat16((unsigned short)(b >> 16));
   }
@@ -103,7 +103,7 @@ struct Codec<__nv_bfloat16, float> {
   }
   template <int I>
   __device__ static __forceinline__ __nv_bfloat16 enc(float v, const StepPlan& p) {
-    return encd<I>(v - p.dref[I], p);
+    return encd<I>((v - p.dref[I]) * (float)p.scale, p);
   }
 };
 
@@ -174,7 +174,7 @@ __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, i
 }
 
 // A stored population as the step kernels carry it: the full value, or for the 16-bit tiers
-// its deviation from the storage reference.  dref is symmetric (dref_i = dref_opp(i)), so an
+// its scaled deviation from the storage reference (the stored number itself).  dref is symmetric (dref_i = dref_opp(i)), so an
 // on-node bounce-back reads the opposite slot with the same meaning.
 template <typename S, typename R, int I>
 __device__ __forceinline__ R load_value(S raw, const StepPlan& p) {
@@ -319,10 +319,10 @@ __device__ __forceinline__ constexpr int mrt_den(int k) {
                           : (k == 9 ? (I >= 15 ? 18 : 36) : (k == 10 ? (I >= 15 ? 36 : 72) : MrtTables::BD_DIAG[k])));
 }
 
-// DEVF: v holds deviations from the storage reference (the MRT rest state, whose moments are
-// rho0, e = -11 rho0, eps = w_eps rho0 and zero otherwise).  The moments of v are then the
-// deviations of the moments, the e / eps equilibria take the density deviation m[0], and only the
-// force term needs the full density rho0 + m[0].
+// DEVF: v holds scaled deviations from the storage reference (the MRT rest state, whose moments
+// are rho0, e = -11 rho0, eps = w_eps rho0 and zero otherwise).  The moments of v are then the
+// scaled deviations of the moments, the e / eps equilibria take the density deviation m[0], the
+// quadratic equilibrium terms take one factor 1/scale, and the force term the full density.
 template <typename R, bool STRICT, bool DEVF = false>
 __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
   R m[19];
@@ -346,16 +346,20 @@ __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
   const R s1 = R(p.mrt[0]), s2 = R(p.mrt[1]), s4 = R(p.mrt[2]), s10 = R(p.mrt[3]), s16 = R(p.mrt[4]);
   const R weps = R(p.mrt[5]), wepsj = R(p.mrt[6]), wxx = R(p.mrt[7]);
   const R rho0 = R(1.);
-  const R jx2 = jx * jx, jy2 = jy * jy, jz2 = jz * jz;
+  // DEVF: scaled deviation moments; a product of two scaled momenta carries one scale too many
+  const R qs = DEVF ? R(p.inv_scale) : R(1);
+  const R jxq = DEVF ? jx * qs : jx;
+  const R jyq = DEVF ? jy * qs : jy;
+  const R jx2 = jxq * jx, jy2 = jyq * jy, jz2 = (DEVF ? jz * qs : jz) * jz;
   const R jj = (jx2 + jy2 + jz2);
   // relaxation (mrt.hpp:103-126), rho0 = 1
   const R e_eq = R(-11) * rho + R(19) / rho0 * jj;
   const R eps_eq = weps * rho + wepsj / rho0 * jj;
   const R pxx3_eq = R(1) / (rho0) * (R(2) * jx2 - (jy2 + jz2));
   const R pww_eq = R(1) / rho0 * (jy2 - jz2);
-  const R pxy_eq = R(1) / rho0 * jx * jy;
-  const R pyz_eq = R(1) / rho0 * jy * jz;
-  const R pxz_eq = R(1) / rho0 * jx * jz;
+  const R pxy_eq = R(1) / rho0 * jxq * jy;
+  const R pyz_eq = R(1) / rho0 * jyq * jz;
+  const R pxz_eq = R(1) / rho0 * jxq * jz;
   R mo[19];
   mo[0] = rho;
   mo[1] = e - s1 * (e - e_eq);
@@ -394,7 +398,8 @@ __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
         first = false;
       }
     });
-    if (force) acc = acc + R(3.) * (DEVF ? R(p.rho0) + rho : rho) * weight<R, I>() * edot<I, R>(Fx, Fy, Fz);
+    if (force)
+      acc = acc + R(3.) * (DEVF ? R(p.scale) * (R(p.rho0) + rho * qs) : rho) * weight<R, I>() * edot<I, R>(Fx, Fy, Fz);
     v[I] = acc;
   });
 }
@@ -590,34 +595,36 @@ __device__ __forceinline__ void collide(R (&v)[Q], const StepPlan& p) {
     mrt<R, STRICT>(v, p);
 }
 
-// BGK on deviations d_i = f_i - w_i rho0 (the BGK storage reference): rho = rho0 + sum d,
-// j = sum e d, feq_i - w_i rho0 = w_i (rho - rho0) + w_i rho (3 e.u + 4.5 (e.u)^2 - 1.5 u^2).
+// BGK on scaled deviations v_i = scale * (f_i - w_i rho0) (w_i rho0 is the BGK storage reference):
+// rho = rho0 + sum v / scale, u = (sum e v) / (scale rho), and per direction
+// v_i <- (1 - 1/tau) v_i + (1/tau) w_i (sum v + scale rho P_i), P_i = e.u (3 + 4.5 e.u) - 1.5 u^2.
 // Every sum runs over small numbers, so FP32 keeps the deviations' own precision and its rounding
 // does not accumulate into the mass the way a sum of full populations does.
 template <typename R>
 __device__ __forceinline__ void bgk_dev(R (&v)[Q], const StepPlan& p) {
-  R drho = v[0];
+  R drs = v[0];
 #pragma unroll
-  for (int i = 1; i < Q; i++) drho = drho + v[i];
-  R ux = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
-  R uy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
-  R uz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
-  const R rho = R(p.rho0) + drho;
-  const R inv = R(1) / rho;
-  ux *= inv;
-  uy *= inv;
-  uz *= inv;
-  const R u_squ = (ux * ux + uy * uy + uz * uz);
-  const R inv_tau = R(p.inv_tau);
-  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  for (int i = 1; i < Q; i++) drs = drs + v[i];
+  const R jx = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
+  const R jy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
+  const R jz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
+  const R rho = R(p.rho0) + drs * R(p.inv_scale);
+  const R srho = R(p.scale) * rho;
+  const R cu = R(1) / srho;
+  const R ux = jx * cu, uy = jy * cu, uz = jz * cu;
+  const R c15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+  const R om = R(p.inv_tau), om1 = R(1) - om;
   const bool force = p.has_force != 0;
+  const R f3 = R(3.) * srho;
+  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
   Unroll<0, Q>::run([&]<int I>() {
     constexpr R w = weight<R, I>();
     const R eu = edot<I, R>(ux, uy, uz);
-    const R feqd = w * drho + w * rho * (R(3.) * eu + R(4.5) * eu * eu - R(1.5) * u_squ);
-    R d = (feqd - v[I]) * inv_tau;
-    if (force) d += R(3.) * rho * w * edot<I, R>(Fx, Fy, Fz);
-    v[I] += d;
+    const R P = eu * (R(3.) + R(4.5) * eu) - c15;
+    const R feq = w * (drs + srho * P);
+    R out = om1 * v[I] + om * feq;
+    if (force) out += w * f3 * edot<I, R>(Fx, Fy, Fz);
+    v[I] = out;
   });
 }
 
@@ -631,22 +638,24 @@ __device__ __forceinline__ void collide_dev(R (&v)[Q], const StepPlan& p) {
 
 // Everything after the gather: boundary operators on the nodes whose values were pulled
 // (`pulled` false for a first step, which collides the initial state), start_iteration boxes,
-// collision.  The 16-bit tiers carry deviations; the boundary operators and the boxes work on
-// full populations, so those nodes convert around them.
+// collision.  The 16-bit tiers carry scaled deviations; the boundary operators and the boxes work
+// on full populations, so those nodes convert around them.
 template <typename S, typename R, bool STRICT, int MODE, int COLL>
 __device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin, int64_t idx, int x, int y, int z,
                                             int8_t flag, const StepPlan& p, bool pulled, bool edge) {
   constexpr bool DEV = is_16bit<S>();
   if (pulled && edge && p.nops > 0) {
-    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] += R(p.dref[I]); });
+    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] = fmaf(v[I], R(p.inv_scale), R(p.dref[I])); });
     plane_ops<S, R>(v, fin, idx, x, y, z, flag, p);
-    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] -= R(p.dref[I]); });
+    if constexpr (DEV) Unroll<0, Q>::run([&]<int I>() { v[I] = (v[I] - R(p.dref[I])) * R(p.scale); });
   }
   if (MODE != MODE_FINISH) {
     for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
       const SetBox& b = p.sets[s];
       if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
-        Unroll<0, Q>::run([&]<int I>() { v[I] = R(b.value) * weight<R, I>() - (DEV ? R(p.dref[I]) : R(0)); });
+        Unroll<0, Q>::run([&]<int I>() {
+          v[I] = DEV ? (R(b.value) * weight<R, I>() - R(p.dref[I])) * R(p.scale) : R(b.value) * weight<R, I>();
+        });
     }
     if (flag == FLAG_FLUID) {
       if constexpr (DEV)
@@ -694,16 +703,18 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
       sy[k] = cy;
       sz[k] = cz;
     }
+    // every load is issued before any value is used; a bounced value (the node's own opp(I)
+    // slot) decodes like a pulled one because the storage reference is symmetric
+    S raw[Q];
     Unroll<0, Q>::run([&]<int I>() {
       constexpr int kx = 1 - D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
       constexpr int O = D3Q19::opp(I);
       bool bounce = ox[kx] || oy[ky] || oz[kz];
       const int64_t src = ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx + sx[kx];
       if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
-      const S* ptr = bounce ? fin + O * p.stride + idx : fin + I * p.stride + src;
-      const S raw = ld_stream(ptr);
-      v[I] = bounce ? load_value<S, R, O>(raw, p) : load_value<S, R, I>(raw, p);
+      raw[I] = ld_stream(bounce ? fin + O * p.stride + idx : fin + I * p.stride + src);
     });
+    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(raw[I], p); });
   }
   const bool edge = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
   node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, edge);

@@ -75,6 +75,11 @@ const char* hlbm_version(void);
 int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],
                 int32_t precision, int32_t device, hlbm_ctx** out);
 int hlbm_destroy(hlbm_ctx* ctx);
+/* Device memory of contexts and batches comes from a stream-ordered pool per device that keeps
+ * freed blocks for the next allocation, so that creating and destroying lattices while others run
+ * costs no device-wide synchronisation (no reference counterpart).  hlbm_trim_memory waits for the
+ * device and returns the pool's unused blocks to the driver. */
+int hlbm_trim_memory(int32_t device);
 
 /* lbm_parameters (lbm_parameters.cpp:73-99): tau if has_tau, else dt if dt > 0, else the
  * celerity defines the lattice time step; Fext is converted to lattice units. */
@@ -211,8 +216,8 @@ void* hlbm_stream(hlbm_ctx* ctx);
  * and boundary operators -- with ONE launch of the pipelined persistent kernel per time step, over
  * the concatenated tile list of all members; steps are replayed from a captured CUDA graph of two
  * steps.  Kernel (hlbm_batch_tune): tiles of about 256 nodes with direct pulls, any lattice
- * shape -- 8 (default) a persistent grid of resident CTAs each walking a contiguous range of tiles,
- * 9 one CTA per tile; 6 / 7 = the pipelined kernel
+ * shape -- 8 (default) one CTA per tile, 9 a persistent grid of resident CTAs each walking a
+ * contiguous range of tiles; 6 / 7 = the pipelined kernel
  * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0).  A
  * member that has not stepped yet takes its first step inside the batched launch.  While a
  * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.  A lattice
