@@ -68,6 +68,7 @@ def parse_args():
     ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,bf16",
                     help="precision workload: storage tiers (\":nearest\": round-to-nearest storage)")
     ap.add_argument("--members", type=int, default=256, help="batch workload: lattices")
+    ap.add_argument("--batch-variant", type=int, default=8, help="batch and serve workloads: hlbm_batch_tune variant")
     ap.add_argument("--member-steps", type=int, default=2000, help="batch workload: steps of every lattice")
     ap.add_argument("--alone-steps", type=int, default=200,
                     help="batch workload: steps per lattice of the one-at-a-time comparison")
@@ -369,6 +370,7 @@ def run_batch(a):
     lats = [Lattice.from_case(c, "f32") for c in cases]
     nodes = sum(l.ncell for l in lats)
     batch = Batch("f32")
+    batch.tune(a.batch_variant)
     for l in lats:
         batch.add(l)
     stream = torch.cuda.ExternalStream(batch.stream_handle(), device=torch.device("cuda", 0))
@@ -409,7 +411,7 @@ def run_batch(a):
             "steps": timed, "warmup": a.warmup, "ms_per_step": round(ms / timed, 4), "higher_is_better": True,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"mixed_batch_{a.members}", "members": a.members, "nodes": nodes,
-                       "kinds": kinds, "seed": 20261203, "kernel_variant": 8},
+                       "kinds": kinds, "seed": 20261203, "kernel_variant": a.batch_variant},
             "one_at_a_time_mlups": round(alone, 1), "speedup_vs_one_at_a_time": round(mlups / alone, 2),
             "gpu_launches": info["launches"] - info0["launches"], "graph_replays": info["graph_replays"] - info0["graph_replays"],
             "clocks": clk}
@@ -422,7 +424,8 @@ def run_serve(a):
 
     lines = []
     for rate in [float(r) for r in a.rates.split(",")]:
-        fast = serve.serve_batched(serve.make_stream(rate, a.requests), "f16", hbm_budget=160e9)
+        fast = serve.serve_batched(serve.make_stream(rate, a.requests), "f16", hbm_budget=160e9,
+                                   variant=a.batch_variant)
         plain = serve.serve_plain(serve.make_stream(rate, a.requests), "f64")
         lines.append({"rate": rate, "batched_f16": fast, "plain_f64": plain,
                       "mlups_ratio": round(fast["aggregate_mlups"] / plain["aggregate_mlups"], 2)})

@@ -30,7 +30,8 @@ class Batch:
         return self
 
     def tune(self, variant: int):
-        """8: one CTA per tile (default); 9: persistent tile walk; 6 / 7: pipelined kernel."""
+        """8: one CTA per tile (default); 9: persistent tile walk; 6 / 7: pipelined kernel;
+        10: every member's own single-lattice kernel, run concurrently from one captured graph."""
         capi.check(self.L.hlbm_batch_tune(self.h, int(variant)))
         return self
 

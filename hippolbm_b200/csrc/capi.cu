@@ -143,6 +143,10 @@ struct hlbm_ctx {
   int* err_dev = nullptr;
   int ntiles = 0, tile_elems = 0, tma_stages = 0, tma_stages2 = 0, sms = 148;
   hlbm_batch* batch = nullptr;  // the batch this lattice is a member of
+  int64_t plan_version = 0;       // bumped whenever the step plan is rebuilt
+  uint32_t* seed_dev = nullptr;   // step-number pair of graph-replayed launches (16-bit tiers)
+  uint32_t seed_host[2] = {0, 0};
+  cudaEvent_t join_ev = nullptr;  // end of this member's work in a concurrent batch graph
 };
 
 namespace {
@@ -345,6 +349,7 @@ int build_plan(hlbm_ctx* c) {
   }
   if (int rc = setup_pipeline(c)) return rc;
   c->plan_dirty = false;
+  c->plan_version++;
   return HLBM_OK;
 }
 
@@ -359,11 +364,12 @@ cudaError_t outlet_passes(int prec, const StepPlan& p, const LatticeDesc* descs,
   return cudaSuccess;
 }
 
-cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fout, int variant) {
-  c->plan.seed = uint32_t(c->steps);  // the step number salts the stochastic rounding
-  const StepPlan& p = c->plan;
+// One step (or read-out) of lattice c with plan p on stream s: the outlet passes, then the step
+// kernel of `variant`.
+cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout, const StepPlan& p, int variant,
+                             cudaStream_t s) {
   if (mode != MODE_PROLOGUE)  // the descriptor holds f[0], f[1] with cur = 0
-    if (cudaError_t e = outlet_passes(c->precision, p, c->desc_dev, 0, fin == c->f[0] ? 0 : 1, c->n, c->stream,
+    if (cudaError_t e = outlet_passes(c->precision, p, c->desc_dev, 0, fin == c->f[0] ? 0 : 1, c->n, s,
                                       c->launches))
       return e;
   const int walls = p.walls;
@@ -378,15 +384,20 @@ cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fo
   t.parity = (fin == c->f[0]) ? 0 : 1;
   t.err = c->err_dev;
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
-  t.seed = c->steps;
+  t.seed = p.seed;
   c->launches++;
   switch (c->precision) {
-    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
-    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
-    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
-    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
-    default: return step_bf16(mode, walls, fin, fout, c->flags, p, c->stream, variant, t);
+    case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
+    case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, s, variant, t);
+    case HLBM_F32: return step_f32(mode, walls, fin, fout, c->flags, p, s, variant, t);
+    case HLBM_F16: return step_f16(mode, walls, fin, fout, c->flags, p, s, variant, t);
+    default: return step_bf16(mode, walls, fin, fout, c->flags, p, s, variant, t);
   }
+}
+
+cudaError_t launch_step_variant(hlbm_ctx* c, int mode, const void* fin, void* fout, int variant) {
+  c->plan.seed = uint32_t(c->steps);  // the step number salts the stochastic rounding
+  return launch_with_plan(c, mode, fin, fout, c->plan, variant, c->stream);
 }
 
 // a pipelined-kernel wait that timed out leaves a code in the device error word
@@ -533,10 +544,11 @@ int hlbm_destroy(hlbm_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) {  // the memory returns to the pool once the stream's work is done
     void* bufs[] = {c->f[0], c->f[1], c->flags, c->partials, c->stats_dev, c->plane_tmp, c->uprev,
-                    c->plan_dev, c->desc_dev, c->tiles_dev, c->err_dev};
+                    c->plan_dev, c->desc_dev, c->tiles_dev, c->err_dev, c->seed_dev};
     for (void* b : bufs) pool_free(b, c->stream);
     cudaStreamDestroy(c->stream);
   }
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
   delete c;
   return HLBM_OK;
 }
@@ -1185,6 +1197,12 @@ struct hlbm_batch {
   int* err_dev = nullptr;
   cudaGraphExec_t graph = nullptr;  // two steps: parity 0 then parity 1
   int64_t replays = 0, launches = 0;
+  // variant 10 (concurrent): a captured graph of two steps of every member, and what it was
+  // captured for (members, their buffer parity and plan versions)
+  cudaGraphExec_t cgraph = nullptr;
+  cudaEvent_t fork_ev = nullptr;
+  std::vector<hlbm_ctx*> cg_members;
+  std::vector<int64_t> cg_state;
 };
 
 namespace {
@@ -1194,6 +1212,119 @@ int batch_fail(int code, const std::string& m) { return fail(code, m); }
 void batch_drop_graph(hlbm_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
+  if (b->cgraph) cudaGraphExecDestroy(b->cgraph);
+  b->cgraph = nullptr;
+  b->cg_members.clear();
+  b->cg_state.clear();
+}
+
+// ------------------------------------------------------------------ concurrent batches (variant 10)
+// Every member steps with its own single-lattice kernel (its plan in kernel parameters, the
+// collision specialised, vectorised where eligible); the members' launches are forked onto their
+// own streams so that small lattices run side by side, and two steps of all of them are replayed
+// from one captured graph.  Graph-replayed launches of the 16-bit tiers read their step number
+// (the stochastic-rounding salt) from a per-member device counter pair, so every member rounds
+// exactly as it does stepped alone.
+int concurrent_variant(const hlbm_ctx* c) { return c->variant < 6 ? c->variant : 4; }
+
+int64_t concurrent_state(const hlbm_ctx* c) { return (c->plan_version * 2 + c->cur) * 16 + concurrent_variant(c); }
+
+int batch_capture_concurrent(hlbm_batch* b) {
+  if (b->cgraph) cudaGraphExecDestroy(b->cgraph);
+  b->cgraph = nullptr;
+  const bool sr = b->precision == HLBM_F16 || b->precision == HLBM_BF16;
+  if (!b->fork_ev) HLBM_CK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+  for (hlbm_ctx* c : b->members) {
+    if (!c->join_ev) HLBM_CK(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
+    if (sr && !c->seed_dev) {
+      if (pool_alloc((void**)&c->seed_dev, 2 * sizeof(uint32_t), c->device, c->stream) != cudaSuccess)
+        return fail(HLBM_ENOMEM, "hlbm_batch_step: step counters");
+      HLBM_CK(cudaStreamSynchronize(c->stream));
+    }
+  }
+  cudaGraph_t g = nullptr;
+  HLBM_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaEventRecord(b->fork_ev, b->stream);
+  for (hlbm_ctx* c : b->members) {
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, b->fork_ev, 0);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+      StepPlan pk = c->plan;
+      pk.seed_dev = sr ? c->seed_dev : nullptr;
+      pk.seed_parity = k;
+      e = launch_with_plan(c, MODE_FUSED, c->f[c->cur ^ k], c->f[c->cur ^ k ^ 1], pk, concurrent_variant(c), c->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(c->join_ev, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, c->join_ev, 0);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return fail(HLBM_ECUDA, "hlbm_batch_step: capture of the concurrent graph failed");
+  }
+  const cudaError_t e3 = cudaGraphInstantiate(&b->cgraph, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) return fail(HLBM_ECUDA, "hlbm_batch_step: graph instantiation failed");
+  b->cg_members = b->members;
+  b->cg_state.clear();
+  for (hlbm_ctx* c : b->members) b->cg_state.push_back(concurrent_state(c));
+  return HLBM_OK;
+}
+
+int batch_step_concurrent(hlbm_batch* b, int64_t nsteps) {
+  const bool sr = b->precision == HLBM_F16 || b->precision == HLBM_BF16;
+  bool fresh = false;
+  for (hlbm_ctx* c : b->members) {
+    if (int rc = build_plan(c)) return rc;
+    if (c->phase == MATER) c->phase = POSTCOL;
+    fresh |= c->phase == RAW;
+    HLBM_CK(cudaStreamSynchronize(c->stream));
+  }
+  auto direct_step = [&]() -> int {  // one step of every member, launched on its own stream
+    for (hlbm_ctx* c : b->members) {
+      const int mode = c->phase == RAW ? MODE_PROLOGUE : MODE_FUSED;
+      HLBM_CK(launch_step_variant(c, mode, c->f[c->cur], c->f[1 - c->cur], concurrent_variant(c)));
+      c->cur = 1 - c->cur;
+      c->phase = POSTCOL;
+      c->steps++;
+      b->launches++;
+    }
+    for (hlbm_ctx* c : b->members) HLBM_CK(cudaStreamSynchronize(c->stream));
+    return HLBM_OK;
+  };
+  int64_t todo = nsteps;
+  if (fresh) {
+    if (int rc = direct_step()) return rc;
+    todo--;
+  }
+  if (todo >= 2) {
+    bool valid = b->cgraph && b->cg_members == b->members;
+    for (size_t m = 0; valid && m < b->members.size(); m++)
+      valid = b->cg_state[m] == concurrent_state(b->members[m]);
+    if (!valid)
+      if (int rc = batch_capture_concurrent(b)) return rc;
+    if (sr) {  // the counters start at each member's own step count
+      for (hlbm_ctx* c : b->members) {
+        c->seed_host[0] = uint32_t(c->steps);
+        c->seed_host[1] = uint32_t(c->steps + 1);
+        HLBM_CK(cudaMemcpyAsync(c->seed_dev, c->seed_host, sizeof(c->seed_host), cudaMemcpyHostToDevice, c->stream));
+      }
+      for (hlbm_ctx* c : b->members) HLBM_CK(cudaStreamSynchronize(c->stream));
+    }
+    while (todo >= 2) {
+      HLBM_CK(cudaGraphLaunch(b->cgraph, b->stream));
+      b->replays++;
+      b->launches += 2 * int64_t(b->members.size());
+      for (hlbm_ctx* c : b->members) c->steps += 2;
+      todo -= 2;
+    }
+    HLBM_CK(cudaStreamSynchronize(b->stream));
+  }
+  if (todo == 1)
+    if (int rc = direct_step()) return rc;
+  for (hlbm_ctx* c : b->members)
+    if (int rc = check_device_error(c)) return rc;
+  return HLBM_OK;
 }
 
 // rebuild the concatenated tile list and the descriptors of the members
@@ -1347,6 +1478,7 @@ int hlbm_batch_add(hlbm_batch* b, hlbm_ctx* c) {
   b->members.push_back(c);
   c->batch = b;
   b->dirty = true;
+  batch_drop_graph(b);  // an in-flight replay still completes
   return HLBM_OK;
 }
 
@@ -1358,6 +1490,7 @@ int hlbm_batch_remove(hlbm_batch* b, hlbm_ctx* c) {
       b->members.erase(b->members.begin() + m);
       c->batch = nullptr;
       b->dirty = true;
+      batch_drop_graph(b);
       return HLBM_OK;
     }
   return fail(HLBM_EINVAL, "hlbm_batch_remove: lattice not in the batch");
@@ -1367,6 +1500,7 @@ int hlbm_batch_step(hlbm_batch* b, int64_t nsteps) {
   if (!b || nsteps < 0) return fail(HLBM_EINVAL, "hlbm_batch_step: bad argument");
   if (nsteps == 0 || b->members.empty()) return HLBM_OK;
   HLBM_CK(cudaSetDevice(b->device));
+  if (b->variant == 10) return batch_step_concurrent(b, nsteps);
   b->descs_stale = true;  // members may have been read out or rewritten since the last call
   bool fresh = false;
   for (hlbm_ctx* c : b->members) {
@@ -1430,7 +1564,8 @@ int hlbm_batch_step(hlbm_batch* b, int64_t nsteps) {
 }
 
 int hlbm_batch_tune(hlbm_batch* b, int32_t variant) {
-  if (!b || variant < 6 || variant > 9) return fail(HLBM_EINVAL, "hlbm_batch_tune: variant must be 6, 7, 8 or 9");
+  if (!b || variant < 6 || variant > 10)
+    return fail(HLBM_EINVAL, "hlbm_batch_tune: variant must be 6, 7, 8, 9 or 10");
   if (variant < 8)
     for (hlbm_ctx* c : b->members)
       if ((size_t(c->n[0]) * elem_size(c->precision)) % 16 != 0)
@@ -1474,6 +1609,7 @@ int hlbm_batch_destroy(hlbm_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (hlbm_ctx* c : b->members) c->batch = nullptr;
   batch_drop_graph(b);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->stream) {
     pool_free(b->desc_dev, b->stream);
     pool_free(b->tiles_dev, b->stream);

@@ -65,6 +65,10 @@ struct StepPlan {
   float dref[Q];      // 16-bit storage keeps (f_i - dref_i) * scale; dref_i = feq_i(rho0, u0)
   uint32_t seed;      // step number of the launch: salt of the stochastic rounding
   int32_t rounding;   // 16-bit storage: 0 round to nearest, 1 stochastic rounding
+  // when set, the step number comes from seed_dev[seed_parity] instead of `seed`, and the launch
+  // writes seed_dev[seed_parity ^ 1] = that + 1 (launches replayed from a captured graph)
+  uint32_t* seed_dev;
+  int32_t seed_parity;
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };

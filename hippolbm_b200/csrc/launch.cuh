@@ -75,7 +75,8 @@ cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const S
 }
 
 // Step kernel variants 0..5: variant % 2 selects the kernel (0: one node per thread, 1:
-// vectorised when eligible), variant / 2 the occupancy target: at least 1, 2 or 3 blocks of 256
+// vectorised when eligible, else one node per thread at 3 blocks/SM), variant / 2 the occupancy
+// target: at least 1, 2 or 3 blocks of 256
 // threads per SM (__launch_bounds__ minimum blocks, which caps registers at 255, 128 or 85 per
 // thread).  Variants 6 and 7: the bulk-copy pipelined persistent kernel (lbm_step_tma.cuh), with
 // tiles of about 512 (variant 6) or 1024 (variant 7) nodes; fused steps only, when eligible.
@@ -179,6 +180,7 @@ cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const 
     variant = 4;
   }
   const bool vec = (variant % 2) == 1 && vec_eligible<S>(p, walls);
+  if ((variant % 2) == 1 && !vec) variant = 4;  // no vectorised kernel for this lattice: 3 CTAs/SM scalar
   switch (variant / 2) {
     case 0: return launch_minb<S, R, STRICT, 1>(mode, walls, vec, fin, fout, flags, p, s);
     case 1: return launch_minb<S, R, STRICT, 2>(mode, walls, vec, fin, fout, flags, p, s);

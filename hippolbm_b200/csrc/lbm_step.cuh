@@ -160,10 +160,10 @@ struct Unroll<N, N> {
 // carried (MODE_PROLOGUE / MODE_FUSED with p.rounding), else to nearest.  The branch is taken
 // once per node: selecting per value would make the compiler evaluate both conversions.
 template <typename S, typename R, int MODE, class Dst>
-__device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, int64_t idx, Dst&& dst) {
+__device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, uint32_t seed, int64_t idx, Dst&& dst) {
   if constexpr (is_16bit<S>()) {
     if (MODE != MODE_FINISH && p.rounding) {
-      const uint32_t h = node_hash(idx, p.seed);
+      const uint32_t h = node_hash(idx, seed);
       Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd_sr<I>(v[I], p, dir_bits<I>(h))); });
     } else {
       Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd<I>(v[I], p)); });
@@ -171,6 +171,23 @@ __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, i
   } else {
     Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc<I>(v[I], p)); });
   }
+}
+
+// The launch's step number (the stochastic-rounding salt): from the plan, or from the device
+// counter pair of a graph-replayed launch (see StepPlan::seed_dev).
+template <typename S>
+__device__ __forceinline__ uint32_t launch_seed(const StepPlan& p) {
+  if constexpr (is_16bit<S>())
+    if (p.seed_dev) return p.seed_dev[p.seed_parity];
+  return p.seed;
+}
+
+// One thread of the grid moves the counter pair on: no block of this launch reads the other slot.
+template <typename S, int MODE>
+__device__ __forceinline__ void advance_seed(const StepPlan& p) {
+  if constexpr (is_16bit<S>() && MODE != MODE_FINISH)
+    if (p.seed_dev && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+      p.seed_dev[p.seed_parity ^ 1] = p.seed_dev[p.seed_parity] + 1u;
 }
 
 // A stored population as the step kernels carry it: the full value, or for the 16-bit tiers
@@ -718,13 +735,14 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
   }
   const bool edge = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
   node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, edge);
-  store_node<S, R, MODE>(v, p, idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
+  store_node<S, R, MODE>(v, p, launch_seed<S>(p), idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
 }
 
 // ------------------------------------------------------------------ the step kernel
 template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout,
                                                     const int8_t* __restrict__ flags, const StepPlan p) {
+  advance_seed<S, MODE>(p);
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;

@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
       });
       node_update<S, R, STRICT, MODE_FUSED, 2>(v, fin, idx, x, y, z, flag, p, !first,
                                                x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1);
-      store_node<S, R, MODE_FUSED>(v, p, idx, [&]<int I>(S s) { fout[I * stride + idx] = s; });
+      store_node<S, R, MODE_FUSED>(v, p, p.seed, idx, [&]<int I>(S s) { fout[I * stride + idx] = s; });
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s

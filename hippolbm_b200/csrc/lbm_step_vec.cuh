@@ -184,6 +184,8 @@ __device__ __forceinline__ void load_flags(const int8_t* p, int8_t (&fl)[NPT]) {
 template <typename S, typename R, bool STRICT, int MODE, int NPT, int COLL, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fin, S* __restrict__ fout,
                                                      const int8_t* __restrict__ flags, const StepPlan p) {
+  advance_seed<S, MODE>(p);
+  const uint32_t seed = launch_seed<S>(p);
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;  // vector index along x
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
     Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(c[I].template get<K>(), p); });
     node_update<S, R, STRICT, MODE, COLL>(v, fin, row + x, x, yy, z, fl[K], p, MODE != MODE_PROLOGUE,
                                           yz_face || x == 0 || x == p.nx - 1);
-    store_node<S, R, MODE>(v, p, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
+    store_node<S, R, MODE>(v, p, seed, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
   });
   Unroll<0, Q>::run([&]<int I>() { c[I].store(fout + I * p.stride + row + x0); });
 }

@@ -117,13 +117,17 @@ def _stats(reqs: list[Request], t_end: float, precision: str, mode: str) -> dict
 
 
 def serve_batched(requests: list[Request], precision: str = "f16", device: int = 0, hbm_budget: float = 160e9,
-                  chunk: int = 100, check_every: int = 500, clock=time.perf_counter, keep_results: bool = False) -> dict:
-    """Continuous batching: admit while memory allows, advance all admitted solves together."""
+                  chunk: int = 100, check_every: int = 500, clock=time.perf_counter, keep_results: bool = False,
+                  variant: int | None = None) -> dict:
+    """Continuous batching: admit while memory allows, advance all admitted solves together
+    (`variant`: the batch kernel, hlbm_batch_tune)."""
     pending = sorted(requests, key=lambda r: r.arrival)
     active: list[Request] = []
     finished: list[Request] = []
     used = 0
     batch = Batch(precision, device)
+    if variant is not None:
+        batch.tune(variant)
     start = clock()
     try:
         while pending or active:
@@ -163,7 +167,9 @@ def serve_batched(requests: list[Request], precision: str = "f16", device: int =
             if r.lat is not None:
                 r.lat.close()
         batch.close()
-    return _stats(finished, clock() - start, precision, "continuous batching")
+    out = _stats(finished, clock() - start, precision, "continuous batching")
+    out["batch_variant"] = 8 if variant is None else variant
+    return out
 
 
 def serve_plain(requests: list[Request], precision: str = "f64", device: int = 0, chunk: int = 100,

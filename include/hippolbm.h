@@ -218,7 +218,10 @@ void* hlbm_stream(hlbm_ctx* ctx);
  * steps.  Kernel (hlbm_batch_tune): tiles of about 256 nodes with direct pulls, any lattice
  * shape -- 8 (default) one CTA per tile, 9 a persistent grid of resident CTAs each walking a
  * contiguous range of tiles; 6 / 7 = the pipelined kernel
- * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0).  A
+ * (rows bulk-copied into shared memory; members need nx * bytes per population % 16 == 0);
+ * 10 = no shared launch: every member runs its own single-lattice step kernel (its hlbm_tune
+ * variant, 4 for 6 / 7) on its own stream, all members forked from and joined to the batch stream
+ * inside one captured graph of two steps.  A
  * member that has not stepped yet takes its first step inside the batched launch.  While a
  * lattice is in a batch, step it only through hlbm_batch_step; read-outs stay valid.  A lattice
  * belongs to at most one batch; hlbm_destroy of a member removes it from its batch first.

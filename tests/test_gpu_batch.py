@@ -47,7 +47,7 @@ def carried(case, flags):
 
 
 @pytest.mark.parametrize("precision", ["f64_strict", "f32"])
-@pytest.mark.parametrize("variant", [8, 9, 6])
+@pytest.mark.parametrize("variant", [8, 9, 6, 10])
 def test_batch_members_equal_their_runs_alone(precision, variant):
     from hippolbm_b200.batch import Batch
     from hippolbm_b200.lattice import Lattice
@@ -141,6 +141,44 @@ def test_f16_members_equal_their_batch_of_one(variant):
                 b1.add(one)
                 b1.step(n)
                 b1.remove(one)
+            f1 = one.populations()
+            m = carried(case, one.flags())
+        assert np.array_equal(f[:, m], f1[:, m]), case.name
+
+
+@pytest.mark.parametrize("precision", ["f16", "bf16"])
+def test_concurrent_members_equal_their_runs_alone(precision):
+    """Variant 10 steps every member with its own single-lattice kernel, forked onto the members'
+    streams inside one captured graph; graph-replayed launches read the stochastic-rounding step
+    number from a device counter.  Each member ends bit for bit where it ends stepped alone, through
+    joins, an odd step count and a rounding-mode change that forces a new capture."""
+    from hippolbm_b200.batch import Batch
+    from hippolbm_b200.lattice import Lattice
+
+    lats = [Lattice.from_case(c, precision) for c in CASES]
+    with Batch(precision) as b:
+        b.tune(10)
+        for lat in lats[:3]:
+            b.add(lat)
+        b.step(5)
+        for lat in lats[3:]:
+            b.add(lat)
+        b.step(12)
+        lats[1].rounding("nearest")
+        b.step(4)
+        assert b.info()["graph_replays"] >= 8
+        out = [(lat.info()["steps"], lat.populations()) for lat in lats]
+        for lat in lats:
+            b.remove(lat)
+    for i, (case, lat, (n, f)) in enumerate(zip(CASES, lats, out)):
+        lat.close()
+        with Lattice.from_case(case, precision) as one:
+            if i == 1:
+                one.step(17)
+                one.rounding("nearest")
+                one.step(n - 17)
+            else:
+                one.step(n)
             f1 = one.populations()
             m = carried(case, one.flags())
         assert np.array_equal(f[:, m], f1[:, m]), case.name
