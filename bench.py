@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_POP = {"f64": 8, "f64_strict": 8, "f32": 4, "f16": 2, "bf16": 2}
+DEFAULT_VARIANT = {"f64": 4, "f64_strict": 4, "f32": 5, "f16": 5, "bf16": 5}
 DTYPE = {"f64": "f64", "f64_strict": "f64", "f32": "f32", "f16": "f32 (f16 storage)", "bf16": "f32 (bf16 storage)"}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -59,7 +60,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=500, help="time steps per end-to-end solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=128, help="lattice edge of the CPU baseline sample")
-    ap.add_argument("--variant", type=int, default=-1, help="step-kernel variant; -1: autotune")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="step-kernel variant; -1: the tier's default (4 for FP64, 5 for FP32 and 16-bit)")
+    ap.add_argument("--autotune", action="store_true", help="time every variant on the lattice and keep the fastest")
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="16-bit storage rounding")
     ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve"])
@@ -164,13 +167,21 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_node(precision: str, collision: str):
-    """DRAM bytes per node per launch of the fused step from the committed ncu summary."""
+def step_kernel_name(variant: int) -> str:
+    """The fused step kernel a single-lattice variant runs on a lattice without wall obstacles
+    whose rows split into at least 32 vectors (the Couette workload)."""
+    if variant >= 6:
+        return "k_step_tma"
+    return "k_step_vec" if variant % 2 == 1 else "k_step"
+
+
+def ncu_traffic_per_node(precision: str, collision: str, kernel: str):
+    """DRAM bytes per node per launch of the fused step kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as fh:
             d = json.load(fh)
-        return float(d[f"{precision}_{collision}"]["dram_bytes_per_node"])
+        return float(d[f"{precision}_{collision}_{kernel}"]["dram_bytes_per_node"])
     except (OSError, KeyError, ValueError):
         return None
 
@@ -232,12 +243,13 @@ def run_ours(a):
     lat.rounding(a.rounding)
     stream = torch.cuda.ExternalStream(lat.stream_handle(), device=device)
     nodes = lat.ncell
-    # the project's autotuner picks the step-kernel variant on this lattice (state unchanged)
-    if a.variant >= 0:
-        variant, variant_ms = a.variant, {}
-        lat.tune(variant)
-    else:
+    # the tier's default step-kernel variant (the autotuner's pick on this workload), or the
+    # autotuner's pick on this lattice (state unchanged)
+    if a.autotune:
         variant, variant_ms = lat.autotune(reps=3)
+    else:
+        variant, variant_ms = (a.variant if a.variant >= 0 else DEFAULT_VARIANT[a.precision]), {}
+        lat.tune(variant)
     # warm-up
     lat.step(a.warmup)
     lat.sync()
@@ -302,11 +314,12 @@ def run_ours(a):
         alg_bytes_per_node = 38 * bpp + 1
         achieved = nodes * alg_bytes_per_node / (ms_per_step * 1e-3) / 1e9
         peak, peak_kind = measured_hbm_peak()
-        tpn = ncu_traffic_per_node(a.precision, a.collision)
+        kname = step_kernel_name(variant)
+        tpn = ncu_traffic_per_node(a.precision, a.collision, kname)
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
                 "traffic": round(tpn * nodes) if tpn else None,
-                "algorithmic_bytes_per_node": alg_bytes_per_node, "kernel": "hlbm::k_step (MODE_FUSED)"}
+                "algorithmic_bytes_per_node": alg_bytes_per_node, "kernel": f"hlbm::{kname} (MODE_FUSED)"}
         cpu = None
         if not a.no_cpu_baseline and world == 1:
             cpu_steps = 10

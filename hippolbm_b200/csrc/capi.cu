@@ -202,6 +202,10 @@ void base_plan(hlbm_ctx* c, StepPlan& p) {
   storage_reference(c, p.dref);
   p.rounding = c->rounding;
   p.seed = uint32_t(c->steps);
+  const int bx = p.nx < 128 ? ((p.nx + 31) / 32) * 32 : 128;  // row geometry (launch.cuh)
+  const bool idle_lanes = ((p.nx + bx - 1) / bx) * bx != p.nx;
+  p.linear = (idle_lanes && int64_t(p.nx) * p.ny < (int64_t(1) << 24)) ? 1 : 0;
+  p.inv_nx = 1.0f / float(p.nx);
 }
 
 // the box {int(min / dx), int(max / dx)} of set_distribution / update_obstacles in real
@@ -386,6 +390,9 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
   t.seed = p.seed;
   c->launches++;
+  if (variant < 6 && variant % 2 == 1 && vec_eligible_bytes(p, walls, int(elem_size(c->precision))) &&
+      mode != MODE_PROLOGUE && face_pass_mask(p) != 0)
+    c->launches++;  // the face pass after the vectorised kernel
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
     case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, s, variant, t);
@@ -497,8 +504,8 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
   c->stride = (c->ncell + 127) / 128 * 128;
   if (precision == HLBM_F16) c->scale = 1024.0;
   // default step-kernel variant per tier, from hlbm_autotune on 512^3 Couette (B200): FP64 one
-  // node per thread at >= 3 blocks/SM; FP32 vectorised at >= 3; FP16/BF16 vectorised at >= 2
-  c->variant = (precision == HLBM_F32) ? 5 : ((precision == HLBM_F16 || precision == HLBM_BF16) ? 3 : 4);
+  // node per thread at >= 3 blocks/SM; FP32, FP16 and BF16 vectorised at >= 3 blocks/SM
+  c->variant = (precision == HLBM_F64 || precision == HLBM_F64_STRICT) ? 4 : 5;
   mrt_reference(c->mrt);
   auto cleanup = [&](int rc) {
     hlbm_destroy(c);
@@ -1203,6 +1210,8 @@ struct hlbm_batch {
   cudaEvent_t fork_ev = nullptr;
   std::vector<hlbm_ctx*> cg_members;
   std::vector<int64_t> cg_state;
+  int64_t cg_kernels = 0;
+  std::vector<int64_t> cg_member_kernels;
 };
 
 namespace {
@@ -1243,6 +1252,8 @@ int batch_capture_concurrent(hlbm_batch* b) {
     }
   }
   cudaGraph_t g = nullptr;
+  std::vector<int64_t> launches_before;
+  for (hlbm_ctx* c : b->members) launches_before.push_back(c->launches);
   HLBM_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaEventRecord(b->fork_ev, b->stream);
   for (hlbm_ctx* c : b->members) {
@@ -1257,6 +1268,14 @@ int batch_capture_concurrent(hlbm_batch* b) {
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, c->join_ev, 0);
   }
   const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  b->cg_kernels = 0;  // kernels of one replay, per member and in all (the capture launched none)
+  b->cg_member_kernels.clear();
+  for (size_t m = 0; m < b->members.size(); m++) {
+    const int64_t k = b->members[m]->launches - launches_before[m];
+    b->members[m]->launches = launches_before[m];
+    b->cg_member_kernels.push_back(k);
+    b->cg_kernels += k;
+  }
   if (e != cudaSuccess || e2 != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
@@ -1314,8 +1333,11 @@ int batch_step_concurrent(hlbm_batch* b, int64_t nsteps) {
     while (todo >= 2) {
       HLBM_CK(cudaGraphLaunch(b->cgraph, b->stream));
       b->replays++;
-      b->launches += 2 * int64_t(b->members.size());
-      for (hlbm_ctx* c : b->members) c->steps += 2;
+      b->launches += b->cg_kernels;
+      for (size_t m = 0; m < b->members.size(); m++) {
+        b->members[m]->steps += 2;
+        b->members[m]->launches += b->cg_member_kernels[m];
+      }
       todo -= 2;
     }
     HLBM_CK(cudaStreamSynchronize(b->stream));

@@ -69,8 +69,39 @@ struct StepPlan {
   // writes seed_dev[seed_parity ^ 1] = that + 1 (launches replayed from a captured graph)
   uint32_t* seed_dev;
   int32_t seed_parity;
+  // geometry of the one-node-per-thread kernel: 0 = x on threadIdx.x, y on threadIdx.y (rows of
+  // whole warps); 1 = blocks of 256 consecutive nodes of a z-plane, for rows that would leave
+  // lanes idle (x = i mod nx, y = i / nx through inv_nx and one correction; planes < 2^24 nodes)
+  int32_t linear;
+  float inv_nx;
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };
+
+// Nodes per thread of the vectorised step kernel for a storage type of `bytes` bytes (one 8-byte
+// vector per direction plane for 2- and 4-byte types, double2 for FP64), and whether a lattice
+// can use it: no wall obstacles, whole vectors per row and at least one warp of them.
+inline constexpr int vec_npt_bytes(int bytes) { return bytes == 2 ? 4 : 2; }
+inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes) {
+  const int npt = vec_npt_bytes(bytes);
+  return !walls && p.nx % npt == 0 && p.nx / npt >= 32;
+}
+
+// Faces whose nodes the boundary operators of the plan can change: every non-periodic face for
+// post_bounce_back, the operator's own face for neumann / lid_driven_cavity.  Bit F = face F
+// (x0, xl, y0, yl, z0, zl).
+inline int face_pass_mask(const StepPlan& p) {
+  int m = 0;
+  for (int o = 0; o < p.nops; o++) {
+    const PlaneOp& op = p.ops[o];
+    if (op.kind == OP_POST_BB) {
+      for (int f = 0; f < 6; f++)
+        if (!p.periodic[f / 2]) m |= 1 << f;
+    } else if (op.kind == OP_ZOUHE || op.kind == OP_LID) {
+      m |= 1 << op.face;
+    }
+  }
+  return m;
+}
 
 }  // namespace hlbm

@@ -11,8 +11,14 @@
 namespace hlbm {
 
 // Geometry of a step launch: x along threadIdx.x (coalesced SoA rows), y on threadIdx.y,
-// z on blockIdx.z.  256 threads per block.
+// z on blockIdx.z; or, for a plan with `linear` set, 256 consecutive nodes of a z-plane per
+// block and z on blockIdx.y.  256 threads per block.
 inline void step_geometry(const StepPlan& p, dim3& grid, dim3& block) {
+  if (p.linear) {
+    block = dim3(256, 1, 1);
+    grid = dim3(unsigned((int64_t(p.nx) * p.ny + 255) / 256), p.nz, 1);
+    return;
+  }
   int bx = 128;
   if (p.nx < 128) bx = ((p.nx + 31) / 32) * 32;
   int by = 256 / bx;
@@ -39,13 +45,12 @@ cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const S
 // 4- and 2-byte storage types (float2, 4 x FP16/BF16); FP64 uses double2
 template <typename S>
 constexpr int vec_npt() {
-  return sizeof(S) == 8 ? 2 : (sizeof(S) == 4 ? 2 : 4);
+  return vec_npt_bytes(int(sizeof(S)));
 }
 
 template <typename S>
 bool vec_eligible(const StepPlan& p, int walls) {
-  constexpr int NPT = vec_npt<S>();
-  return !walls && p.nx % NPT == 0 && p.nx / NPT >= 32;
+  return vec_eligible_bytes(p, walls, int(sizeof(S)));
 }
 
 inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, dim3& block) {
@@ -71,6 +76,23 @@ cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const S
     k_step_vec<S, R, STRICT, MODE, NPT, 1, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   else
     k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+  if (cudaError_t e = cudaGetLastError()) return e;
+  const int faces = face_pass_mask(p);
+  if (MODE == MODE_PROLOGUE || faces == 0) return cudaSuccess;
+  // the face pass: nodes the boundary operators touch, recomputed whole by the scalar node step
+  int64_t area = 0;
+  for (int f = 0; f < 6; f++)
+    if (faces >> f & 1) {
+      const int64_t a = f < 2 ? int64_t(p.ny) * p.nz : (f < 4 ? int64_t(p.nx) * p.nz : int64_t(p.nx) * p.ny);
+      area = a > area ? a : area;
+    }
+  const dim3 fgrid(unsigned((area + 255) / 256), 6, 1);
+  if (MODE == MODE_FUSED && p.collision == 0)
+    k_faces<S, R, STRICT, MODE, 0><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
+  else if (MODE == MODE_FUSED)
+    k_faces<S, R, STRICT, MODE, 1><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
+  else
+    k_faces<S, R, STRICT, MODE, 2><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
   return cudaGetLastError();
 }
 

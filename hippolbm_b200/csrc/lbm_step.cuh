@@ -29,6 +29,32 @@ namespace hlbm {
 
 enum StepMode : int { MODE_PROLOGUE = 0, MODE_FUSED = 1, MODE_FINISH = 2 };
 
+// ------------------------------------------------------------------ 16-bit conversions
+// Two FP32 values to one packed pair (hi in the upper 16 bits).  .rs is sm_100a's stochastic
+// rounding: the discarded bits of each value get a random addend before truncation, from the
+// low (lo) and high (hi) half-word of rbits (13 bits each for FP16, 16 for BF16); .rn rounds
+// to nearest even.
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float hi, float lo, uint32_t rbits) {
+  uint32_t d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+  return d;
+}
+__device__ __forceinline__ uint32_t cvt_rs_bf16x2(float hi, float lo, uint32_t rbits) {
+  uint32_t d;
+  asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+  return d;
+}
+__device__ __forceinline__ uint32_t cvt_rn_f16x2(float hi, float lo) {
+  uint32_t d;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+__device__ __forceinline__ uint32_t cvt_rn_bf16x2(float hi, float lo) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+
 // ------------------------------------------------------------------ storage codecs
 // Populations are stored as S and computed in R.  Half-precision storage keeps the
 // deviation (f_i - w_i * rho0) * scale, so that the stored numbers are small and their
@@ -63,13 +89,18 @@ struct Codec<__half, float> {
   __device__ static __forceinline__ __half encd(float d, const StepPlan&) {
     return __float2half_rn(d);
   }
-  // stochastic rounding: the 13 FP32 mantissa bits below FP16's last bit get a random addend
-  // (the top 13 bits of r), then the value is truncated; Inf / NaN pass unchanged
+  // stochastic rounding of one value (the low half of a pair) and of a pair (lo, hi)
   template <int I>
   __device__ static __forceinline__ __half encd_sr(float d, const StepPlan&, uint32_t r) {
-    uint32_t b = __float_as_uint(d);
-    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 19;
-    return __float2half_rz(__uint_as_float(b));
+    return __ushort_as_half((unsigned short)(cvt_rs_f16x2(0.0f, d, r) & 0xffffu));
+  }
+  template <int I>
+  __device__ static __forceinline__ uint32_t encd_sr2(float lo, float hi, uint32_t r) {
+    return cvt_rs_f16x2(hi, lo, r);
+  }
+  template <int I>
+  __device__ static __forceinline__ uint32_t encd2(float lo, float hi) {
+    return cvt_rn_f16x2(hi, lo);
   }
   template <int I>
   __device__ static __forceinline__ float dec(__half s, const StepPlan& p) {
@@ -90,12 +121,17 @@ struct Codec<__nv_bfloat16, float> {
   __device__ static __forceinline__ __nv_bfloat16 encd(float d, const StepPlan&) {
     return __float2bfloat16_rn(d);
   }
-  // stochastic rounding: a random addend to the 16 discarded bits, then truncation
   template <int I>
   __device__ static __forceinline__ __nv_bfloat16 encd_sr(float d, const StepPlan&, uint32_t r) {
-    uint32_t b = __float_as_uint(d);
-    if ((b & 0x7F800000u) != 0x7F800000u) b += r >> 16;
-    return __ushort_as_bfloat16((unsigned short)(b >> 16));
+    return __ushort_as_bfloat16((unsigned short)(cvt_rs_bf16x2(0.0f, d, r) & 0xffffu));
+  }
+  template <int I>
+  __device__ static __forceinline__ uint32_t encd_sr2(float lo, float hi, uint32_t r) {
+    return cvt_rs_bf16x2(hi, lo, r);
+  }
+  template <int I>
+  __device__ static __forceinline__ uint32_t encd2(float lo, float hi) {
+    return cvt_rn_bf16x2(hi, lo);
   }
   template <int I>
   __device__ static __forceinline__ float dec(__nv_bfloat16 s, const StepPlan& p) {
@@ -128,11 +164,13 @@ __device__ __forceinline__ uint32_t node_hash(int64_t idx, uint32_t seed) {
   return h;
 }
 
-// bits for direction I: the high bits of the node hash times a per-direction odd constant
+// bits for direction I: the node hash times a per-direction odd constant, whose well-mixed high
+// half is folded into the low half, so that both 16-bit halves are usable random bits
 template <int I>
 __device__ __forceinline__ uint32_t dir_bits(uint32_t h) {
   constexpr uint32_t K = 0x9E3779B9u * (2u * I + 1u);
-  return h * K;
+  const uint32_t r = h * K;
+  return r ^ (r >> 16);
 }
 
 template <typename S>
@@ -170,6 +208,21 @@ __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, u
     }
   } else {
     Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template enc<I>(v[I], p)); });
+  }
+}
+
+// Stores the Q values of two x-neighbours a (node idx, low half) and b (node idx + 1, high half)
+// of a 16-bit tier as packed pairs dst(I, word): one conversion per direction and pair, the
+// random bits hashed from the pair's first node.
+template <typename S, typename R, int MODE, class Dst>
+__device__ __forceinline__ void store_pair(const R (&a)[Q], const R (&b)[Q], const StepPlan& p, uint32_t seed,
+                                           int64_t idx, Dst&& dst) {
+  static_assert(is_16bit<S>(), "packed pairs are 16-bit storage");
+  if (MODE != MODE_FINISH && p.rounding) {
+    const uint32_t h = node_hash(idx, seed);
+    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd_sr2<I>(a[I], b[I], dir_bits<I>(h))); });
+  } else {
+    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd2<I>(a[I], b[I])); });
   }
 }
 
@@ -625,24 +678,31 @@ __device__ __forceinline__ void bgk_dev(R (&v)[Q], const StepPlan& p) {
   const R jx = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
   const R jy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
   const R jz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
-  const R rho = R(p.rho0) + drs * R(p.inv_scale);
+  // every product that meets an addition is an explicit fmaf or a __fmul_rn, which the compiler
+  // never contracts: the kernels that inline this code round identically
+  const R rho = fmaf(drs, R(p.inv_scale), R(p.rho0));
   const R srho = R(p.scale) * rho;
   const R cu = R(1) / srho;
-  const R ux = jx * cu, uy = jy * cu, uz = jz * cu;
-  const R c15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+  const R ux = __fmul_rn(jx, cu), uy = __fmul_rn(jy, cu), uz = __fmul_rn(jz, cu);
+  const R c15 = R(1.5) * fmaf(ux, ux, fmaf(uy, uy, __fmul_rn(uz, uz)));
   const R om = R(p.inv_tau), om1 = R(1) - om;
-  const bool force = p.has_force != 0;
-  const R f3 = R(3.) * srho;
-  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  // feq_i / w_i = drs + srho P_i = base + eu (s3 + s45 eu)
+  const R base = fmaf(-srho, c15, drs);
+  const R s3 = R(3.) * srho, s45 = R(4.5) * srho;
+  const R omw[3] = {om * weight<R, 0>(), om * weight<R, 1>(), om * weight<R, 7>()};
   Unroll<0, Q>::run([&]<int I>() {
-    constexpr R w = weight<R, I>();
-    const R eu = edot<I, R>(ux, uy, uz);
-    const R P = eu * (R(3.) + R(4.5) * eu) - c15;
-    const R feq = w * (drs + srho * P);
-    R out = om1 * v[I] + om * feq;
-    if (force) out += w * f3 * edot<I, R>(Fx, Fy, Fz);
-    v[I] = out;
+    constexpr int wc = I == 0 ? 0 : (I < 7 ? 1 : 2);
+    R g = base;
+    if constexpr (I != 0) {
+      const R eu = edot<I, R>(ux, uy, uz);
+      g = fmaf(eu, fmaf(eu, s45, s3), base);
+    }
+    v[I] = fmaf(omw[wc], g, __fmul_rn(om1, v[I]));
   });
+  if (p.has_force != 0) {
+    const R Fx = __fmul_rn(s3, R(p.F[0])), Fy = __fmul_rn(s3, R(p.F[1])), Fz = __fmul_rn(s3, R(p.F[2]));
+    Unroll<1, Q>::run([&]<int I>() { v[I] = fmaf(weight<R, I>(), edot<I, R>(Fx, Fy, Fz), v[I]); });
+  }
 }
 
 template <typename R, int COLL>
@@ -671,7 +731,10 @@ __device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin
       const SetBox& b = p.sets[s];
       if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
         Unroll<0, Q>::run([&]<int I>() {
-          v[I] = DEV ? (R(b.value) * weight<R, I>() - R(p.dref[I])) * R(p.scale) : R(b.value) * weight<R, I>();
+          if constexpr (DEV)
+            v[I] = (__fmul_rn(R(b.value), weight<R, I>()) - R(p.dref[I])) * R(p.scale);
+          else
+            v[I] = R(b.value) * weight<R, I>();
         });
     }
     if (flag == FLAG_FLUID) {
@@ -743,11 +806,49 @@ template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, i
 __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout,
                                                     const int8_t* __restrict__ flags, const StepPlan p) {
   advance_seed<S, MODE>(p);
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= p.nx || y >= p.ny) return;
+  int x, y, z;
+  if (p.linear) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.nx * p.ny) return;
+    z = blockIdx.y;
+    y = __float2int_rz(float(i) * p.inv_nx);  // i / nx within one (exact below 2^24, see StepPlan)
+    x = i - y * p.nx;
+    if (x < 0) {
+      y--;
+      x += p.nx;
+    } else if (x >= p.nx) {
+      y++;
+      x -= p.nx;
+    }
+  } else {
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z = blockIdx.z;
+    if (x >= p.nx || y >= p.ny) return;
+  }
   node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
+}
+
+// The face pass of the vectorised kernels: the nodes of the faces in `faces` (bit F = face F),
+// each stepped whole by node_step, after the vectorised kernel stepped them without boundary
+// operators.  Both read only fin, so the pass overwrites those nodes' outputs with the complete
+// update.  blockIdx.y is the face; nodes on two faces are computed twice, to the same bits.
+template <typename S, typename R, bool STRICT, int MODE, int COLL>
+__global__ void __launch_bounds__(256) k_faces(const S* __restrict__ fin, S* __restrict__ fout,
+                                               const int8_t* __restrict__ flags, const StepPlan p, int faces) {
+  const int F = blockIdx.y;
+  if (!(faces >> F & 1)) return;
+  const int axis = F / 2;
+  const int na = axis == 0 ? p.ny : p.nx;  // the face's two axes, in x, y, z order
+  const int nb = axis == 2 ? p.ny : p.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na * nb) return;
+  const int a = i % na, b = i / na;
+  const int c = (F & 1) ? (axis == 0 ? p.nx : (axis == 1 ? p.ny : p.nz)) - 1 : 0;
+  const int x = axis == 0 ? c : a;
+  const int y = axis == 1 ? c : (axis == 0 ? a : b);
+  const int z = axis == 2 ? c : b;
+  node_step<S, R, STRICT, MODE, false, COLL>(fin, fout, flags, p, x, y, z);
 }
 
 }  // namespace hlbm

@@ -8,6 +8,9 @@
 // it comes from a warp shuffle, and lanes at a warp edge fetch it with one scalar load (the
 // element of the previous/next warp, or the periodic image / on-node bounce-back at a row
 // end).  Warps never straddle rows: the x extent of a block is a multiple of 32 threads.
+// The kernel applies no boundary operator: the launcher follows it with the face pass (k_faces),
+// which recomputes the nodes of the faces those operators touch, so the per-node code here stays
+// small.  The 16-bit tiers update the nodes in pairs whose values convert into packed words.
 #pragma once
 #include "lbm_step.cuh"
 
@@ -263,15 +266,29 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
   if (!valid) return;
   int8_t fl[NPT];
   load_flags<NPT>(flags + row + x0, fl);
-  const bool yz_face = yy == 0 || z == 0 || yy == p.ny - 1 || z == p.nz - 1;
-  Unroll<0, NPT>::run([&]<int K>() {
-    const int x = x0 + K;
-    R v[Q];
-    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(c[I].template get<K>(), p); });
-    node_update<S, R, STRICT, MODE, COLL>(v, fin, row + x, x, yy, z, fl[K], p, MODE != MODE_PROLOGUE,
-                                          yz_face || x == 0 || x == p.nx - 1);
-    store_node<S, R, MODE>(v, p, seed, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
-  });
+  if constexpr (is_16bit<S>()) {
+    // node pairs (2j, 2j+1): the two values of a direction convert into one packed word
+    Unroll<0, NPT / 2>::run([&]<int J>() {
+      constexpr int K0 = 2 * J, K1 = 2 * J + 1;
+      const int xa = x0 + K0, xb = x0 + K1;
+      R a[Q], b[Q];
+      Unroll<0, Q>::run([&]<int I>() {
+        a[I] = load_value<S, R, I>(c[I].template get<K0>(), p);
+        b[I] = load_value<S, R, I>(c[I].template get<K1>(), p);
+      });
+      node_update<S, R, STRICT, MODE, COLL>(a, fin, row + xa, xa, yy, z, fl[K0], p, false, false);
+      node_update<S, R, STRICT, MODE, COLL>(b, fin, row + xb, xb, yy, z, fl[K1], p, false, false);
+      store_pair<S, R, MODE>(a, b, p, seed, row + xa, [&]<int I>(uint32_t w) { c[I].w[J] = w; });
+    });
+  } else {
+    Unroll<0, NPT>::run([&]<int K>() {
+      const int x = x0 + K;
+      R v[Q];
+      Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(c[I].template get<K>(), p); });
+      node_update<S, R, STRICT, MODE, COLL>(v, fin, row + x, x, yy, z, fl[K], p, false, false);
+      store_node<S, R, MODE>(v, p, seed, row + x, [&]<int I>(S s) { c[I].template set<K>(s); });
+    });
+  }
   Unroll<0, Q>::run([&]<int I>() { c[I].store(fout + I * p.stride + row + x0); });
 }
 
