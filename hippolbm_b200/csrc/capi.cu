@@ -351,6 +351,7 @@ int build_plan(hlbm_ctx* c) {
     }
     b.value = h.value;
   }
+  p.face_mask = face_pass_mask(p);
   if (int rc = setup_pipeline(c)) return rc;
   c->plan_dirty = false;
   c->plan_version++;

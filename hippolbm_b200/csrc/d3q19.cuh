@@ -74,6 +74,7 @@ struct StepPlan {
   // lanes idle (x = i mod nx, y = i / nx through inv_nx and one correction; planes < 2^24 nodes)
   int32_t linear;
   float inv_nx;
+  int32_t face_mask;  // face_pass_mask of the plan: faces whose nodes the boundary operators change
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };

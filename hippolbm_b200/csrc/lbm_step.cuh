@@ -713,6 +713,15 @@ __device__ __forceinline__ void collide_dev(R (&v)[Q], const StepPlan& p) {
     mrt<R, false, true>(v, p);
 }
 
+// Whether node (x, y, z) lies on a face whose boundary operators can change it (p.face_mask).
+// Other boundary nodes skip the operator code: for the 16-bit tiers that also skips a conversion
+// to full populations and back, which would round.
+__device__ __forceinline__ bool on_op_face(const StepPlan& p, int x, int y, int z) {
+  const int bits = int(x == 0) | int(x == p.nx - 1) << 1 | int(y == 0) << 2 | int(y == p.ny - 1) << 3 |
+                   int(z == 0) << 4 | int(z == p.nz - 1) << 5;
+  return (bits & p.face_mask) != 0;
+}
+
 // Everything after the gather: boundary operators on the nodes whose values were pulled
 // (`pulled` false for a first step, which collides the initial state), start_iteration boxes,
 // collision.  The 16-bit tiers carry scaled deviations; the boundary operators and the boxes work
@@ -796,8 +805,7 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
     });
     Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(raw[I], p); });
   }
-  const bool edge = x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
-  node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, edge);
+  node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, on_op_face(p, x, y, z));
   store_node<S, R, MODE>(v, p, launch_seed<S>(p), idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
 }
 

@@ -270,8 +270,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
         else
           v[I] = load_value<S, R, I>(row[xs], p);
       });
-      node_update<S, R, STRICT, MODE_FUSED, 2>(v, fin, idx, x, y, z, flag, p, !first,
-                                               x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1);
+      node_update<S, R, STRICT, MODE_FUSED, 2>(v, fin, idx, x, y, z, flag, p, !first, on_op_face(p, x, y, z));
       store_node<S, R, MODE_FUSED>(v, p, p.seed, idx, [&]<int I>(S s) { fout[I * stride + idx] = s; });
     }
     __syncwarp();
