@@ -391,9 +391,8 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
   t.seed = p.seed;
   c->launches++;
-  if (variant < 6 && variant % 2 == 1 && vec_eligible_bytes(p, walls, int(elem_size(c->precision))) &&
-      mode != MODE_PROLOGUE && face_pass_mask(p) != 0)
-    c->launches++;  // the face pass after the vectorised kernel
+  if (face_pass_runs(p, walls, variant, mode == MODE_PROLOGUE, int(elem_size(c->precision))))
+    c->launches++;  // the face pass after the step kernel
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
     case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, s, variant, t);

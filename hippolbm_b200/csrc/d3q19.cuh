@@ -88,6 +88,14 @@ inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes) {
   return !walls && p.nx % npt == 0 && p.nx / npt >= 32;
 }
 
+// Whether a single-lattice launch of step variant `variant` (not the prologue) is followed by the
+// face pass: the vectorised kernel always, the one-node kernel for the 4- and 2-byte tiers; the
+// pipelined kernel (variants 6, 7) applies the operators inline.
+inline bool face_pass_runs(const StepPlan& p, int walls, int variant, bool prologue, int bytes) {
+  if (variant >= 6 || prologue || p.face_mask == 0) return false;
+  return (variant % 2 == 1 && vec_eligible_bytes(p, walls, bytes)) || bytes < 8;
+}
+
 // Faces whose nodes the boundary operators of the plan can change: every non-periodic face for
 // post_bounce_back, the operator's own face for neumann / lid_driven_cavity.  Bit F = face F
 // (x0, xl, y0, yl, z0, zl).

@@ -26,6 +26,28 @@ inline void step_geometry(const StepPlan& p, dim3& grid, dim3& block) {
   grid = dim3((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, p.nz);
 }
 
+// The face pass after a step kernel that left the boundary operators out: the nodes of the faces
+// in p.face_mask, recomputed whole by the one-node step.
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS>
+cudaError_t launch_faces(const S* fi, S* fo, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
+  const int faces = p.face_mask;
+  if (MODE == MODE_PROLOGUE || faces == 0) return cudaSuccess;
+  int64_t area = 0;
+  for (int f = 0; f < 6; f++)
+    if (faces >> f & 1) {
+      const int64_t a = f < 2 ? int64_t(p.ny) * p.nz : (f < 4 ? int64_t(p.nx) * p.nz : int64_t(p.nx) * p.ny);
+      area = a > area ? a : area;
+    }
+  const dim3 fgrid(unsigned((area + 255) / 256), 6, 1);
+  if (MODE == MODE_FUSED && p.collision == 0)
+    k_faces<S, R, STRICT, MODE, WALLS, 0><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
+  else if (MODE == MODE_FUSED)
+    k_faces<S, R, STRICT, MODE, WALLS, 1><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
+  else
+    k_faces<S, R, STRICT, MODE, WALLS, 2><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
+  return cudaGetLastError();
+}
+
 template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int MINB>
 cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
   dim3 grid, block;
@@ -38,7 +60,9 @@ cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const S
     k_step<S, R, STRICT, MODE, WALLS, 1, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   else
     k_step<S, R, STRICT, MODE, WALLS, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
-  return cudaGetLastError();
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if constexpr (face_pass_tier<S>()) return launch_faces<S, R, STRICT, MODE, WALLS>(fi, fo, flags, p, s);
+  return cudaSuccess;
 }
 
 // nodes per thread of the vectorised kernel: one 8-byte vector per direction plane for the
@@ -77,23 +101,7 @@ cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const S
   else
     k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   if (cudaError_t e = cudaGetLastError()) return e;
-  const int faces = face_pass_mask(p);
-  if (MODE == MODE_PROLOGUE || faces == 0) return cudaSuccess;
-  // the face pass: nodes the boundary operators touch, recomputed whole by the scalar node step
-  int64_t area = 0;
-  for (int f = 0; f < 6; f++)
-    if (faces >> f & 1) {
-      const int64_t a = f < 2 ? int64_t(p.ny) * p.nz : (f < 4 ? int64_t(p.nx) * p.nz : int64_t(p.nx) * p.ny);
-      area = a > area ? a : area;
-    }
-  const dim3 fgrid(unsigned((area + 255) / 256), 6, 1);
-  if (MODE == MODE_FUSED && p.collision == 0)
-    k_faces<S, R, STRICT, MODE, 0><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
-  else if (MODE == MODE_FUSED)
-    k_faces<S, R, STRICT, MODE, 1><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
-  else
-    k_faces<S, R, STRICT, MODE, 2><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);
-  return cudaGetLastError();
+  return launch_faces<S, R, STRICT, MODE, false>(fi, fo, flags, p, s);
 }
 
 // Step kernel variants 0..5: variant % 2 selects the kernel (0: one node per thread, 1:

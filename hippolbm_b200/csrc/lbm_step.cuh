@@ -756,8 +756,9 @@ __device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin
 }
 
 // The whole step for the node (x, y, z): gather (pull with periodic wrap and on-node
-// bounce-back), boundary operators, start_iteration boxes, collision, store.
-template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL>
+// bounce-back), boundary operators (unless OPS is false: a face pass applies them), start_iteration
+// boxes, collision, store.
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, bool OPS = true>
 __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restrict__ fout,
                                           const int8_t* __restrict__ flags, const StepPlan& p, int x, int y, int z) {
   const int64_t idx = ((int64_t)z * p.ny + y) * p.nx + x;
@@ -805,8 +806,17 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
     });
     Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(raw[I], p); });
   }
-  node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE, on_op_face(p, x, y, z));
+  node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE,
+                                        OPS && on_op_face(p, x, y, z));
   store_node<S, R, MODE>(v, p, launch_seed<S>(p), idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
+}
+
+// Storage types whose one-node step kernel leaves the boundary operators to the face pass (k_faces):
+// the 4- and 2-byte tiers, whose kernels are bound by instruction issue, so the operator code
+// costs there.  FP64 applies them inline: its kernel runs at the copy bandwidth either way.
+template <typename S>
+constexpr bool face_pass_tier() {
+  return sizeof(S) < 8;
 }
 
 // ------------------------------------------------------------------ the step kernel
@@ -834,14 +844,14 @@ __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S
     z = blockIdx.z;
     if (x >= p.nx || y >= p.ny) return;
   }
-  node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
+  node_step<S, R, STRICT, MODE, WALLS, COLL, !face_pass_tier<S>()>(fin, fout, flags, p, x, y, z);
 }
 
 // The face pass of the vectorised kernels: the nodes of the faces in `faces` (bit F = face F),
 // each stepped whole by node_step, after the vectorised kernel stepped them without boundary
 // operators.  Both read only fin, so the pass overwrites those nodes' outputs with the complete
 // update.  blockIdx.y is the face; nodes on two faces are computed twice, to the same bits.
-template <typename S, typename R, bool STRICT, int MODE, int COLL>
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL>
 __global__ void __launch_bounds__(256) k_faces(const S* __restrict__ fin, S* __restrict__ fout,
                                                const int8_t* __restrict__ flags, const StepPlan p, int faces) {
   const int F = blockIdx.y;
@@ -856,7 +866,7 @@ __global__ void __launch_bounds__(256) k_faces(const S* __restrict__ fin, S* __r
   const int x = axis == 0 ? c : a;
   const int y = axis == 1 ? c : (axis == 0 ? a : b);
   const int z = axis == 2 ? c : b;
-  node_step<S, R, STRICT, MODE, false, COLL>(fin, fout, flags, p, x, y, z);
+  node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
 }
 
 }  // namespace hlbm
