@@ -173,6 +173,20 @@ __device__ __forceinline__ uint32_t dir_bits(uint32_t h) {
   return r ^ (r >> 16);
 }
 
+// Random bits for the pair conversion of direction I from two independent hash words: one IMAD.
+// The high half-word is the well-mixed top of h * K; the low half-word is a bijection of h's low
+// bits plus h2's, so it is uniform and, between two directions, the offset is independent of the
+// value it is added to.
+__device__ __forceinline__ uint32_t second_hash(uint32_t h) {
+  uint32_t g = (h ^ (h >> 15)) * 0x2C1B3C6Du;
+  return g ^ (g >> 12);
+}
+template <int I>
+__device__ __forceinline__ uint32_t pair_bits(uint32_t h, uint32_t h2) {
+  constexpr uint32_t K = 0x9E3779B9u * (2u * I + 1u);
+  return h * K + h2;
+}
+
 template <typename S>
 constexpr bool is_16bit() {
   return sizeof(S) == 2;
@@ -220,7 +234,10 @@ __device__ __forceinline__ void store_pair(const R (&a)[Q], const R (&b)[Q], con
   static_assert(is_16bit<S>(), "packed pairs are 16-bit storage");
   if (MODE != MODE_FINISH && p.rounding) {
     const uint32_t h = node_hash(idx, seed);
-    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd_sr2<I>(a[I], b[I], dir_bits<I>(h))); });
+    const uint32_t h2 = second_hash(h);
+    Unroll<0, Q>::run([&]<int I>() {
+      dst.template operator()<I>(Codec<S, R>::template encd_sr2<I>(a[I], b[I], pair_bits<I>(h, h2)));
+    });
   } else {
     Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd2<I>(a[I], b[I])); });
   }

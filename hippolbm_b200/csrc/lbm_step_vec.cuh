@@ -12,6 +12,8 @@
 // which recomputes the nodes of the faces those operators touch, so the per-node code here stays
 // small.  The 16-bit tiers update the nodes in pairs whose values convert into packed words.
 #pragma once
+#include <type_traits>
+
 #include "lbm_step.cuh"
 
 namespace hlbm {
@@ -111,6 +113,18 @@ struct PackedChunk {
   __device__ __forceinline__ void set(S v) {
     const unsigned b = bits(v);
     w[K / 2] = (K & 1) ? ((w[K / 2] & 0xffffu) | (b << 16)) : ((w[K / 2] & 0xffff0000u) | b);
+  }
+  // both elements of word J as FP32 (the stored numbers: scaled deviations)
+  template <int J>
+  __device__ __forceinline__ void unpack(float& lo, float& hi) const {
+    if constexpr (sizeof(S) == 2 && std::is_same_v<S, __half>) {
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[J]));
+      lo = f.x;
+      hi = f.y;
+    } else {
+      lo = __uint_as_float(w[J] << 16);
+      hi = __uint_as_float(w[J] & 0xffff0000u);
+    }
   }
   __device__ __forceinline__ S first() const { return get<0>(); }
   __device__ __forceinline__ S last() const { return get<NPT - 1>(); }
@@ -272,10 +286,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
       constexpr int K0 = 2 * J, K1 = 2 * J + 1;
       const int xa = x0 + K0, xb = x0 + K1;
       R a[Q], b[Q];
-      Unroll<0, Q>::run([&]<int I>() {
-        a[I] = load_value<S, R, I>(c[I].template get<K0>(), p);
-        b[I] = load_value<S, R, I>(c[I].template get<K1>(), p);
-      });
+      Unroll<0, Q>::run([&]<int I>() { c[I].template unpack<J>(a[I], b[I]); });
       node_update<S, R, STRICT, MODE, COLL>(a, fin, row + xa, xa, yy, z, fl[K0], p, false, false);
       node_update<S, R, STRICT, MODE, COLL>(b, fin, row + xb, xb, yy, z, fl[K1], p, false, false);
       store_pair<S, R, MODE>(a, b, p, seed, row + xa, [&]<int I>(uint32_t w) { c[I].w[J] = w; });
