@@ -88,6 +88,13 @@ inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes) {
   return !walls && p.nx % npt == 0 && p.nx / npt >= 32;
 }
 
+// Whether the 16-bit one-node kernel can run two nodes per thread: even z-planes (every pair on a
+// 4-byte boundary) of fewer than 2^24 nodes.
+inline bool pairs_eligible(const StepPlan& p) {
+  const int64_t plane = int64_t(p.nx) * p.ny;
+  return plane % 2 == 0 && plane < (int64_t(1) << 24);
+}
+
 // Whether a single-lattice launch of step variant `variant` (not the prologue) is followed by the
 // face pass: the vectorised kernel always, the one-node kernel for the 4- and 2-byte tiers; the
 // pipelined kernel (variants 6, 7) applies the operators inline.

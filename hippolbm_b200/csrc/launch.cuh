@@ -54,6 +54,20 @@ cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const S
   step_geometry(p, grid, block);
   const S* fi = static_cast<const S*>(fin);
   S* fo = static_cast<S*>(fout);
+  if constexpr (is_16bit<S>()) {
+    if (pairs_eligible(p)) {  // two nodes per thread, packed stores
+      const int64_t plane = int64_t(p.nx) * p.ny;
+      const dim3 pgrid(unsigned((plane / 2 + 255) / 256), p.nz, 1);
+      if (MODE == MODE_FUSED && p.collision == 0)
+        k_step_pairs<S, R, STRICT, MODE, WALLS, 0, MINB><<<pgrid, 256, 0, s>>>(fi, fo, flags, p);
+      else if (MODE == MODE_FUSED)
+        k_step_pairs<S, R, STRICT, MODE, WALLS, 1, MINB><<<pgrid, 256, 0, s>>>(fi, fo, flags, p);
+      else
+        k_step_pairs<S, R, STRICT, MODE, WALLS, 2, MINB><<<pgrid, 256, 0, s>>>(fi, fo, flags, p);
+      if (cudaError_t e = cudaGetLastError()) return e;
+      return launch_faces<S, R, STRICT, MODE, WALLS>(fi, fo, flags, p, s);
+    }
+  }
   if (MODE == MODE_FUSED && p.collision == 0)
     k_step<S, R, STRICT, MODE, WALLS, 0, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   else if (MODE == MODE_FUSED)

@@ -772,9 +772,49 @@ __device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin
   }
 }
 
-// The whole step for the node (x, y, z): gather (pull with periodic wrap and on-node
-// bounce-back), boundary operators (unless OPS is false: a face pass applies them), start_iteration
-// boxes, collision, store.
+// The stored values the node (x, y, z) gathers (pull with periodic wrap and on-node bounce-back;
+// in the prologue its own values), every load issued before any is used.  A bounced value (the
+// node's own opp(I) slot) decodes like a pulled one because the storage reference is symmetric.
+template <typename S, int MODE, bool WALLS>
+__device__ __forceinline__ void node_gather(const S* __restrict__ fin, const int8_t* __restrict__ flags,
+                                            const StepPlan& p, int x, int y, int z, int64_t idx, S (&raw)[Q]) {
+  if (MODE == MODE_PROLOGUE) {
+    Unroll<0, Q>::run([&]<int I>() { raw[I] = ld_stream(fin + I * p.stride + idx); });
+    return;
+  }
+  // source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others flag "outside"
+  int sx[3], sy[3], sz[3];
+  bool ox[3], oy[3], oz[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int d = 1 - k;  // component of e_i: +1, 0, -1 -> source offset -d
+    int cx = x - d, cy = y - d, cz = z - d;
+    ox[k] = oy[k] = oz[k] = false;
+    if (cx < 0 || cx >= p.nx) {
+      if (p.periodic[0]) cx = cx < 0 ? cx + p.nx : cx - p.nx; else ox[k] = true;
+    }
+    if (cy < 0 || cy >= p.ny) {
+      if (p.periodic[1]) cy = cy < 0 ? cy + p.ny : cy - p.ny; else oy[k] = true;
+    }
+    if (cz < 0 || cz >= p.nz) {
+      if (p.periodic[2]) cz = cz < 0 ? cz + p.nz : cz - p.nz; else oz[k] = true;
+    }
+    sx[k] = cx;
+    sy[k] = cy;
+    sz[k] = cz;
+  }
+  Unroll<0, Q>::run([&]<int I>() {
+    constexpr int kx = 1 - D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
+    constexpr int O = D3Q19::opp(I);
+    bool bounce = ox[kx] || oy[ky] || oz[kz];
+    const int64_t src = ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx + sx[kx];
+    if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
+    raw[I] = ld_stream(bounce ? fin + O * p.stride + idx : fin + I * p.stride + src);
+  });
+}
+
+// The whole step for the node (x, y, z): gather, boundary operators (unless OPS is false: a face
+// pass applies them), start_iteration boxes, collision, store.
 template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, bool OPS = true>
 __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restrict__ fout,
                                           const int8_t* __restrict__ flags, const StepPlan& p, int x, int y, int z) {
@@ -785,44 +825,10 @@ __device__ __forceinline__ void node_step(const S* __restrict__ fin, S* __restri
       Unroll<0, Q>::run([&]<int I>() { fout[I * p.stride + idx] = Codec<S, R>::template enc<I>(R(0), p); });
     return;
   }
+  S raw[Q];
+  node_gather<S, MODE, WALLS>(fin, flags, p, x, y, z, idx, raw);
   R v[Q];
-  if (MODE == MODE_PROLOGUE) {
-    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(ld_stream(fin + I * p.stride + idx), p); });
-  } else {
-    // source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others flag "outside"
-    int sx[3], sy[3], sz[3];
-    bool ox[3], oy[3], oz[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const int d = 1 - k;  // component of e_i: +1, 0, -1 -> source offset -d
-      int cx = x - d, cy = y - d, cz = z - d;
-      ox[k] = oy[k] = oz[k] = false;
-      if (cx < 0 || cx >= p.nx) {
-        if (p.periodic[0]) cx = cx < 0 ? cx + p.nx : cx - p.nx; else ox[k] = true;
-      }
-      if (cy < 0 || cy >= p.ny) {
-        if (p.periodic[1]) cy = cy < 0 ? cy + p.ny : cy - p.ny; else oy[k] = true;
-      }
-      if (cz < 0 || cz >= p.nz) {
-        if (p.periodic[2]) cz = cz < 0 ? cz + p.nz : cz - p.nz; else oz[k] = true;
-      }
-      sx[k] = cx;
-      sy[k] = cy;
-      sz[k] = cz;
-    }
-    // every load is issued before any value is used; a bounced value (the node's own opp(I)
-    // slot) decodes like a pulled one because the storage reference is symmetric
-    S raw[Q];
-    Unroll<0, Q>::run([&]<int I>() {
-      constexpr int kx = 1 - D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
-      constexpr int O = D3Q19::opp(I);
-      bool bounce = ox[kx] || oy[ky] || oz[kz];
-      const int64_t src = ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx + sx[kx];
-      if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
-      raw[I] = ld_stream(bounce ? fin + O * p.stride + idx : fin + I * p.stride + src);
-    });
-    Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(raw[I], p); });
-  }
+  Unroll<0, Q>::run([&]<int I>() { v[I] = load_value<S, R, I>(raw[I], p); });
   node_update<S, R, STRICT, MODE, COLL>(v, fin, idx, x, y, z, flag, p, MODE != MODE_PROLOGUE,
                                         OPS && on_op_face(p, x, y, z));
   store_node<S, R, MODE>(v, p, launch_seed<S>(p), idx, [&]<int I>(S s) { fout[I * p.stride + idx] = s; });
@@ -861,7 +867,58 @@ __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S
     z = blockIdx.z;
     if (x >= p.nx || y >= p.ny) return;
   }
+  // the face pass computes the nodes of operator faces after this kernel (not after a prologue)
+  if (face_pass_tier<S>() && MODE != MODE_PROLOGUE && on_op_face(p, x, y, z)) return;
   node_step<S, R, STRICT, MODE, WALLS, COLL, !face_pass_tier<S>()>(fin, fout, flags, p, x, y, z);
+}
+
+// The one-node step of the 16-bit tiers, two consecutive nodes of a z-plane per thread: each
+// direction's two results convert into one packed word and one 32-bit store (plane sizes even, so
+// every pair starts on a 4-byte boundary; below 2^24 nodes, for the index arithmetic of `linear`).
+// Boundary operators are left to the face pass.  A wall node of a pair stores the read-out value
+// of a wall (population 0); the one-node kernel leaves that slot untouched, and no fluid node
+// reads it either way.
+template <typename S, typename R, bool STRICT, int MODE, bool WALLS, int COLL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_pairs(const S* __restrict__ fin, S* __restrict__ fout,
+                                                          const int8_t* __restrict__ flags, const StepPlan p) {
+  static_assert(is_16bit<S>(), "packed pairs are 16-bit storage");
+  advance_seed<S, MODE>(p);
+  const int plane = p.nx * p.ny;
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= plane) return;
+  const int z = blockIdx.y;
+  int y = __float2int_rz(float(i) * p.inv_nx);  // i / nx, exact after one correction below 2^24
+  int x = i - y * p.nx;
+  if (x < 0) {
+    y--;
+    x += p.nx;
+  } else if (x >= p.nx) {
+    y++;
+    x -= p.nx;
+  }
+  int xb = x + 1, yb = y;
+  if (xb == p.nx) {
+    xb = 0;
+    yb++;
+  }
+  // both nodes on operator faces: the face pass computes them after this kernel
+  if (MODE != MODE_PROLOGUE && on_op_face(p, x, y, z) && on_op_face(p, xb, yb, z)) return;
+  const int64_t idx = int64_t(z) * plane + i;
+  const int8_t fa = flags[idx], fb = flags[idx + 1];
+  S ra[Q], rb[Q];
+  node_gather<S, MODE, WALLS>(fin, flags, p, x, y, z, idx, ra);
+  node_gather<S, MODE, WALLS>(fin, flags, p, xb, yb, z, idx + 1, rb);
+  R a[Q], b[Q];
+  Unroll<0, Q>::run([&]<int I>() {
+    a[I] = load_value<S, R, I>(ra[I], p);
+    b[I] = load_value<S, R, I>(rb[I], p);
+  });
+  node_update<S, R, STRICT, MODE, COLL>(a, fin, idx, x, y, z, fa, p, false, false);
+  node_update<S, R, STRICT, MODE, COLL>(b, fin, idx + 1, xb, yb, z, fb, p, false, false);
+  if (WALLS && fa == FLAG_WALL) Unroll<0, Q>::run([&]<int I>() { a[I] = -R(p.dref[I]) * R(p.scale); });
+  if (WALLS && fb == FLAG_WALL) Unroll<0, Q>::run([&]<int I>() { b[I] = -R(p.dref[I]) * R(p.scale); });
+  store_pair<S, R, MODE>(a, b, p, launch_seed<S>(p), idx,
+                         [&]<int I>(uint32_t w) { *reinterpret_cast<uint32_t*>(fout + I * p.stride + idx) = w; });
 }
 
 // The face pass of the vectorised kernels: the nodes of the faces in `faces` (bit F = face F),

@@ -211,6 +211,12 @@ __global__ void __launch_bounds__(256, MINB) k_step_vec(const S* __restrict__ fi
   const int lane = threadIdx.x & 31;
   const int x0 = tx * NPT;
   const int yy = y < p.ny ? y : p.ny - 1;
+  // a row on an operator face (y or z): the face pass computes all of it after this kernel.  The
+  // condition is uniform over the warp (one row), so no shuffle partner is missing.
+  if (MODE != MODE_PROLOGUE && (p.face_mask >> 2) != 0 &&
+      (((p.face_mask >> 2) & 1) && yy == 0 || ((p.face_mask >> 3) & 1) && yy == p.ny - 1 ||
+       ((p.face_mask >> 4) & 1) && z == 0 || ((p.face_mask >> 5) & 1) && z == p.nz - 1))
+    return;
   const int64_t row = ((int64_t)z * p.ny + yy) * p.nx;
   Chunk<S, NPT> c[Q];
   if (MODE == MODE_PROLOGUE) {
