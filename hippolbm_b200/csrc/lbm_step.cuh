@@ -739,6 +739,11 @@ __device__ __forceinline__ bool on_op_face(const StepPlan& p, int x, int y, int 
   return (bits & p.face_mask) != 0;
 }
 
+// Whether the z-plane z is an operator face (a test that is uniform over a block of a z-plane).
+__device__ __forceinline__ bool on_op_z_face(const StepPlan& p, int z) {
+  return ((p.face_mask >> 4) & 1 && z == 0) || ((p.face_mask >> 5) & 1 && z == p.nz - 1);
+}
+
 // Everything after the gather: boundary operators on the nodes whose values were pulled
 // (`pulled` false for a first step, which collides the initial state), start_iteration boxes,
 // collision.  The 16-bit tiers carry scaled deviations; the boundary operators and the boxes work
@@ -867,8 +872,9 @@ __global__ void __launch_bounds__(256, MINB) k_step(const S* __restrict__ fin, S
     z = blockIdx.z;
     if (x >= p.nx || y >= p.ny) return;
   }
-  // the face pass computes the nodes of operator faces after this kernel (not after a prologue)
-  if (face_pass_tier<S>() && MODE != MODE_PROLOGUE && on_op_face(p, x, y, z)) return;
+  // the face pass computes the operator faces after this kernel (not after a prologue): whole
+  // z-face planes are skipped (a uniform test per block), other face nodes are computed twice
+  if (face_pass_tier<S>() && MODE != MODE_PROLOGUE && on_op_z_face(p, z)) return;
   node_step<S, R, STRICT, MODE, WALLS, COLL, !face_pass_tier<S>()>(fin, fout, flags, p, x, y, z);
 }
 
@@ -901,8 +907,8 @@ __global__ void __launch_bounds__(256, MINB) k_step_pairs(const S* __restrict__ 
     xb = 0;
     yb++;
   }
-  // both nodes on operator faces: the face pass computes them after this kernel
-  if (MODE != MODE_PROLOGUE && on_op_face(p, x, y, z) && on_op_face(p, xb, yb, z)) return;
+  // a z-face plane: the face pass computes it after this kernel
+  if (MODE != MODE_PROLOGUE && on_op_z_face(p, z)) return;
   const int64_t idx = int64_t(z) * plane + i;
   const int8_t fa = flags[idx], fb = flags[idx + 1];
   S ra[Q], rb[Q];
