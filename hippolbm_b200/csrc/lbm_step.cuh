@@ -491,6 +491,119 @@ __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
   });
 }
 
+// Moments of the basis that are even (equal entries for opposite directions) or odd (opposite
+// entries): rho, e, eps and the stress-like moments are even; momenta, heat fluxes and m_x,y,z odd.
+constexpr bool mrt_even(int k) { return k <= 2 || (k >= 9 && k <= 15); }
+constexpr bool mrt_conserved(int k) { return k == 0 || k == 3 || k == 5 || k == 7; }
+
+template <typename R>
+__device__ __forceinline__ R fmar(R a, R b, R c) {
+  if constexpr (sizeof(R) == 4)
+    return fmaf(a, b, c);
+  else
+    return fma(a, b, c);
+}
+
+// The same MRT collision for the FMA tiers, in fewer operations.  Directions 2p-1 and 2p are
+// opposites, so an even moment sums S_p = f_{2p-1} + f_{2p} and an odd one D_p = f_{2p-1} - f_{2p}
+// (about half the terms of the full transform), and the back-transform (the exact inverse of the
+// basis) gives each opposite pair from one even part E_p and one odd part O_p as E_p +- O_p.  Only
+// the non-conserved moments change, so the update is f_i -= sum_k Minv[i][k] dm_k with
+// dm_k = m_k - m_k*, the relaxation of moment k.  Same equilibria and rates as `mrt`; the
+// operation order differs, so results agree with it to rounding.
+template <typename R, bool DEVF>
+__device__ __forceinline__ void mrt_fast(R (&v)[Q], const StepPlan& p) {
+  R S[10], D[10];
+  Unroll<1, 10>::run([&]<int P>() {
+    S[P] = v[2 * P - 1] + v[2 * P];
+    D[P] = v[2 * P - 1] - v[2 * P];
+  });
+  R m[19];
+  Unroll<0, 19>::run([&]<int K>() {
+    constexpr bool EV = mrt_even(K);
+    R acc = R(0);
+    bool first = true;
+    if constexpr (EV) {
+      constexpr int c0 = MrtTables::M[K][0];
+      if constexpr (c0 != 0) {
+        acc = c0 == 1 ? v[0] : R(c0) * v[0];
+        first = false;
+      }
+    }
+    Unroll<1, 10>::run([&]<int P>() {
+      constexpr int c = MrtTables::M[K][2 * P - 1];
+      if constexpr (c != 0) {
+        const R x = EV ? S[P] : D[P];
+        if (first)
+          acc = c == 1 ? x : (c == -1 ? -x : R(c) * x);
+        else
+          acc = c == 1 ? acc + x : (c == -1 ? acc - x : fmar(R(c), x, acc));
+        first = false;
+      }
+    });
+    m[K] = acc;
+  });
+  const R rho = m[0], e = m[1], eps = m[2], jx = m[3], qx = m[4], jy = m[5], qy = m[6], jz = m[7], qz = m[8],
+          pxx3 = m[9], pixx3 = m[10], pww = m[11], piww = m[12], pxy = m[13], pyz = m[14], pxz = m[15];
+  const R s9 = R(p.inv_tau), s13 = s9;
+  const R s1 = R(p.mrt[0]), s2 = R(p.mrt[1]), s4 = R(p.mrt[2]), s10 = R(p.mrt[3]), s16 = R(p.mrt[4]);
+  const R weps = R(p.mrt[5]), wepsj = R(p.mrt[6]), wxx = R(p.mrt[7]);
+  const R qs = DEVF ? R(p.inv_scale) : R(1);
+  const R jxq = DEVF ? jx * qs : jx;
+  const R jyq = DEVF ? jy * qs : jy;
+  const R jx2 = jxq * jx, jy2 = jyq * jy, jz2 = (DEVF ? jz * qs : jz) * jz;
+  const R jj = (jx2 + jy2 + jz2);
+  const R e_eq = R(-11) * rho + R(19) * jj;
+  const R eps_eq = weps * rho + wepsj * jj;
+  const R pxx3_eq = R(2) * jx2 - (jy2 + jz2);
+  const R pww_eq = jy2 - jz2;
+  R dm[19];
+  dm[1] = s1 * (e - e_eq);
+  dm[2] = s2 * (eps - eps_eq);
+  dm[4] = s4 * (qx + R(2.) / R(3.) * jx);
+  dm[6] = s4 * (qy + R(2.) / R(3.) * jy);
+  dm[8] = s4 * (qz + R(2.) / R(3.) * jz);
+  dm[9] = s9 * (pxx3 - pxx3_eq);
+  dm[10] = s10 * (pixx3 - wxx * pxx3_eq);
+  dm[11] = s9 * (pww - pww_eq);
+  dm[12] = s10 * (piww - wxx * pww_eq);
+  dm[13] = s13 * (pxy - jxq * jy);
+  dm[14] = s13 * (pyz - jyq * jz);
+  dm[15] = s13 * (pxz - jxq * jz);
+  dm[16] = s16 * m[16];
+  dm[17] = s16 * m[17];
+  dm[18] = s16 * m[18];
+  // back-transform of the changes: rest direction, then opposite pairs
+  auto part = [&]<int I, bool WANT_EVEN>() {
+    R acc = R(0);
+    bool first = true;
+    Unroll<0, 19>::run([&]<int K>() {
+      constexpr int num = MrtTables::BN[I][K];
+      if constexpr (num != 0 && !mrt_conserved(K) && mrt_even(K) == WANT_EVEN) {
+        constexpr R coef = R(num) / R(mrt_den<I>(K));
+        acc = first ? coef * dm[K] : fmar(coef, dm[K], acc);
+        first = false;
+      }
+    });
+    return acc;
+  };
+  const bool force = p.has_force != 0;
+  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
+  const R frho = R(3.) * (DEVF ? R(p.scale) * (R(p.rho0) + rho * qs) : rho);
+  v[0] = v[0] - part.template operator()<0, true>();
+  Unroll<1, 10>::run([&]<int P>() {
+    constexpr int A = 2 * P - 1, B = 2 * P;
+    const R E = part.template operator()<A, true>();
+    const R O = part.template operator()<A, false>();
+    v[A] = v[A] - (E + O);
+    v[B] = v[B] - (E - O);
+    if (force) {
+      v[A] = fmar(frho * weight<R, A>(), edot<A, R>(Fx, Fy, Fz), v[A]);
+      v[B] = fmar(frho * weight<R, B>(), edot<B, R>(Fx, Fy, Fz), v[B]);
+    }
+  });
+}
+
 // ------------------------------------------------------------------ Zou/He planes
 // neumann_{x,y,z}_{0,l}<19> (neumann.hpp:27-258) as one table per face.
 struct ZouHeFace {
@@ -678,8 +791,10 @@ template <typename R, bool STRICT, int COLL>
 __device__ __forceinline__ void collide(R (&v)[Q], const StepPlan& p) {
   if (COLL == 0 || (COLL == 2 && p.collision == 0))
     bgk<R, STRICT>(v, p);
+  else if constexpr (STRICT)
+    mrt<R, true>(v, p);
   else
-    mrt<R, STRICT>(v, p);
+    mrt_fast<R, false>(v, p);
 }
 
 // BGK on scaled deviations v_i = scale * (f_i - w_i rho0) (w_i rho0 is the BGK storage reference):
@@ -727,7 +842,7 @@ __device__ __forceinline__ void collide_dev(R (&v)[Q], const StepPlan& p) {
   if (COLL == 0 || (COLL == 2 && p.collision == 0))
     bgk_dev<R>(v, p);
   else
-    mrt<R, false, true>(v, p);
+    mrt_fast<R, true>(v, p);
 }
 
 // Whether node (x, y, z) lies on a face whose boundary operators can change it (p.face_mask).
