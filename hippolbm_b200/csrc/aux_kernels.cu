@@ -398,6 +398,36 @@ cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], 
   return cudaGetLastError();
 }
 
+// near[idx] = 1 when a direction of node idx pulls from a wall node (the pull the step kernels
+// replace by on-node bounce-back under wall_bounce_back), with the gather's periodic wrap; pulls
+// from outside a non-periodic face bounce anyway and are not counted.
+__global__ void k_near_wall(const int8_t* __restrict__ flags, int8_t* __restrict__ near, int nx, int ny, int nz,
+                            int px, int py, int pz) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= nx) return;
+  int8_t any = 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const int m = (dx != 0) + (dy != 0) + (dz != 0);
+        if (m == 0 || m == 3) continue;  // D3Q19: the 6 axis and 12 edge neighbours
+        int sx = x + dx, sy = y + dy, sz = z + dz;
+        if (sx < 0 || sx >= nx) { if (!px) continue; sx = sx < 0 ? sx + nx : sx - nx; }
+        if (sy < 0 || sy >= ny) { if (!py) continue; sy = sy < 0 ? sy + ny : sy - ny; }
+        if (sz < 0 || sz >= nz) { if (!pz) continue; sz = sz < 0 ? sz + nz : sz - nz; }
+        if (flags[(int64_t(sz) * ny + sy) * nx + sx] == FLAG_WALL) any = 1;
+      }
+  near[(int64_t(z) * ny + y) * nx + x] = any;
+}
+
+cudaError_t launch_near_wall(const int8_t* flags, int8_t* near, const int n[3], const int periodic[3],
+                             cudaStream_t s) {
+  const dim3 block(n[0] >= 128 ? 128 : ((n[0] + 31) / 32) * 32);
+  const dim3 grid((n[0] + block.x - 1) / block.x, n[1], n[2]);
+  k_near_wall<<<grid, block, 0, s>>>(flags, near, n[0], n[1], n[2], periodic[0], periodic[1], periodic[2]);
+  return cudaGetLastError();
+}
+
 int stats_blocks(int64_t ncell) {
   int64_t b = (ncell + 255) / 256;
   return int(b < 148 * 8 ? b : 148 * 8);

@@ -23,6 +23,8 @@ cudaError_t launch_zero_gradient(int prec, const LatticeDesc* lats, int m, int f
                                  cudaStream_t s);
 cudaError_t launch_rasterize(int8_t* flags, const StepPlan& p, const int lo[3], const int hi[3], double dx,
                              const ObstacleDesc& o, cudaStream_t s);
+cudaError_t launch_near_wall(const int8_t* flags, int8_t* near, const int n[3], const int periodic[3],
+                             cudaStream_t s);
 int stats_blocks(int64_t ncell);
 cudaError_t launch_macro_stats(int prec, const void* f, const int8_t* flags, const StepPlan& p, double* rho,
                                double* u, double* partials, double* out3, cudaStream_t s);

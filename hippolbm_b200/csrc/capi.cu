@@ -123,6 +123,7 @@ struct hlbm_ctx {
   void* f[2] = {nullptr, nullptr};
   int cur = 0;
   int8_t* flags = nullptr;
+  int8_t* nearwall = nullptr;  // per node: some pull comes from a wall node (k_near_wall)
   double* partials = nullptr;
   double* stats_dev = nullptr;
   double* plane_tmp = nullptr;
@@ -188,6 +189,13 @@ void storage_reference(const hlbm_ctx* c, float dref[Q]) {
   for (int i = 0; i < Q; i++) dref[i] = float((i == 0 ? a : (i <= 6 ? b : cc)) * c->rho0);
 }
 
+// the near-wall map after the flags changed (stream-ordered after the change)
+int refresh_near_wall(hlbm_ctx* c) {
+  c->launches++;
+  HLBM_CK(launch_near_wall(c->flags, c->nearwall, c->n, c->periodic, c->stream));
+  return HLBM_OK;
+}
+
 void base_plan(hlbm_ctx* c, StepPlan& p) {
   std::memset(&p, 0, sizeof(p));
   p.nx = c->n[0];
@@ -197,6 +205,7 @@ void base_plan(hlbm_ctx* c, StepPlan& p) {
   p.ncell = c->ncell;
   p.stride = c->stride;
   p.rho0 = c->rho0;
+  p.nearwall = c->nearwall;
   p.scale = c->scale;
   p.inv_scale = 1.0 / c->scale;
   storage_reference(c, p.dref);
@@ -528,13 +537,15 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate the error word"));
   }
   if (pool_alloc((void**)&c->flags, size_t(c->ncell), c->device, c->stream) != cudaSuccess ||
+      pool_alloc((void**)&c->nearwall, size_t(c->ncell), c->device, c->stream) != cudaSuccess ||
       pool_alloc((void**)&c->partials, sizeof(double) * 4 * 148 * 8, c->device, c->stream) != cudaSuccess ||
       pool_alloc((void**)&c->stats_dev, sizeof(double) * 4, c->device, c->stream) != cudaSuccess) {
     cudaGetLastError();
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate flags"));
   }
   // init_obst: every flag FLUIDE_ (-1 = 0xff)
-  if (cudaMemsetAsync(c->flags, 0xff, size_t(c->ncell), c->stream) != cudaSuccess)
+  if (cudaMemsetAsync(c->flags, 0xff, size_t(c->ncell), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->nearwall, 0, size_t(c->ncell), c->stream) != cudaSuccess)
     return cleanup(fail(HLBM_ECUDA, "cudaMemsetAsync failed"));
   // default lbm_parameters slots (lbm_parameters.cpp:57-64)
   const double F0[3] = {0, 0, 0};
@@ -550,7 +561,7 @@ int hlbm_destroy(hlbm_ctx* c) {
   if (c->batch) hlbm_batch_remove(c->batch, c);  // a batch never keeps a destroyed member
   cudaSetDevice(c->device);
   if (c->stream) {  // the memory returns to the pool once the stream's work is done
-    void* bufs[] = {c->f[0], c->f[1], c->flags, c->partials, c->stats_dev, c->plane_tmp, c->uprev,
+    void* bufs[] = {c->f[0], c->f[1], c->flags, c->nearwall, c->partials, c->stats_dev, c->plane_tmp, c->uprev,
                     c->plan_dev, c->desc_dev, c->tiles_dev, c->err_dev, c->seed_dev};
     for (void* b : bufs) pool_free(b, c->stream);
     cudaStreamDestroy(c->stream);
@@ -755,7 +766,7 @@ int hlbm_update_obstacles(hlbm_ctx* c) {
     c->launches++;
     HLBM_CK(launch_rasterize(c->flags, p, lo, hi, c->dx, o, c->stream));
   }
-  return HLBM_OK;
+  return refresh_near_wall(c);
 }
 
 int hlbm_clear_hooks(hlbm_ctx* c) {
@@ -1001,6 +1012,7 @@ int hlbm_put_flags(hlbm_ctx* c, const int8_t* in) {
   if (!c || !in) return fail(HLBM_EINVAL, "hlbm_put_flags: NULL argument");
   if (int rc = set_device(c)) return rc;
   HLBM_CK(cudaMemcpyAsync(c->flags, in, size_t(c->ncell), cudaMemcpyHostToDevice, c->stream));
+  if (int rc = refresh_near_wall(c)) return rc;
   HLBM_CK(cudaStreamSynchronize(c->stream));
   return HLBM_OK;
 }
@@ -1105,6 +1117,7 @@ int hlbm_checkpoint_load(hlbm_ctx* c, const void* host, int64_t bytes) {
   const unsigned char* in = static_cast<const unsigned char*>(host) + sizeof(h);
   const size_t n = size_t(c->ncell), es = elem_size(c->precision);
   HLBM_CK(cudaMemcpyAsync(c->flags, in, n, cudaMemcpyHostToDevice, c->stream));
+  if (int rc = refresh_near_wall(c)) return rc;
   in += n;
   HLBM_CK(cudaMemcpy2DAsync(c->f[c->cur], size_t(c->stride) * es, in, n * es, n * es, Q, cudaMemcpyHostToDevice,
                             c->stream));

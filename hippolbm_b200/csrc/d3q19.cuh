@@ -75,6 +75,9 @@ struct StepPlan {
   int32_t linear;
   float inv_nx;
   int32_t face_mask;  // face_pass_mask of the plan: faces whose nodes the boundary operators change
+  // per node: 1 when some direction pulls from a wall node (k_near_wall); nodes with 0 skip the
+  // wall test of every pull.  Null: test every pull.
+  const int8_t* nearwall;
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };

@@ -923,12 +923,14 @@ __device__ __forceinline__ void node_gather(const S* __restrict__ fin, const int
     sy[k] = cy;
     sz[k] = cz;
   }
+  bool near = true;  // whether some pull may come from a wall node
+  if constexpr (WALLS) near = p.nearwall == nullptr || p.nearwall[idx] != 0;
   Unroll<0, Q>::run([&]<int I>() {
     constexpr int kx = 1 - D3Q19::ex[I], ky = 1 - D3Q19::ey[I], kz = 1 - D3Q19::ez[I];
     constexpr int O = D3Q19::opp(I);
     bool bounce = ox[kx] || oy[ky] || oz[kz];
     const int64_t src = ((int64_t)sz[kz] * p.ny + sy[ky]) * p.nx + sx[kx];
-    if (WALLS && I != 0 && !bounce) bounce = (flags[src] == FLAG_WALL);
+    if (WALLS && I != 0 && !bounce && near) bounce = (flags[src] == FLAG_WALL);
     raw[I] = ld_stream(bounce ? fin + O * p.stride + idx : fin + I * p.stride + src);
   });
 }
