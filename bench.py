@@ -71,6 +71,9 @@ def parse_args():
     ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,bf16",
                     help="precision workload: storage tiers (\":nearest\": round-to-nearest storage)")
     ap.add_argument("--members", type=int, default=256, help="batch workload: lattices")
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "sjf"], help="serve workload: admission order")
+    ap.add_argument("--max-active-nodes", type=int, default=0,
+                    help="serve workload, sjf: admit while the active lattices hold fewer nodes (0: no cap)")
     ap.add_argument("--batch-variant", type=int, default=8, help="batch and serve workloads: hlbm_batch_tune variant")
     ap.add_argument("--member-steps", type=int, default=2000, help="batch workload: steps of every lattice")
     ap.add_argument("--alone-steps", type=int, default=200,
@@ -438,7 +441,8 @@ def run_serve(a):
     lines = []
     for rate in [float(r) for r in a.rates.split(",")]:
         fast = serve.serve_batched(serve.make_stream(rate, a.requests), "f16", hbm_budget=160e9,
-                                   variant=a.batch_variant)
+                                   variant=a.batch_variant, policy=a.policy,
+                                   max_active_nodes=a.max_active_nodes or None)
         plain = serve.serve_plain(serve.make_stream(rate, a.requests), "f64")
         lines.append({"rate": rate, "batched_f16": fast, "plain_f64": plain,
                       "mlups_ratio": round(fast["aggregate_mlups"] / plain["aggregate_mlups"], 2)})

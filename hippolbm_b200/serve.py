@@ -4,7 +4,8 @@ Requests arrive over time (a Poisson stream).  Each is a D3Q19 solve -- lid-driv
 channel with a velocity inlet, or channel around a sphere -- with a step budget and, optionally, a
 steady-state target: the relative L2 change of the velocity field between checks
 (`hlbm_residual`, FP64 on the device) below a tolerance.  The server admits waiting requests in
-arrival order while their HBM footprint fits the budget, keeps their populations resident, and
+arrival order (or, with the "sjf" policy, smallest work first, up to a cap on the active nodes)
+while their HBM footprint fits the budget, keeps their populations resident, and
 advances every admitted lattice together: one batched kernel launch per time step
 (`hlbm_batch_step`), in chunks.  Between chunks it retires finished solves, frees their memory
 and admits new ones, so requests that arrive while others run join the next chunk.  Time to
@@ -116,11 +117,40 @@ def _stats(reqs: list[Request], t_end: float, precision: str, mode: str) -> dict
             "converged": int(sum(1 for r in reqs if r.tol is not None and r.residual < r.tol))}
 
 
+def admit(arrived: list[Request], active: list[Request], used: int, precision: str, hbm_budget: float,
+          policy: str = "fifo", max_active_nodes: int | None = None) -> list[Request]:
+    """The requests to admit now, in order, from those that have arrived (in arrival order).
+
+    "fifo": arrival order while the HBM footprint fits; a request that does not fit blocks the
+    ones behind it.  "sjf": smallest work (nodes x step budget) first, skipping requests that do
+    not fit, and, with `max_active_nodes`, only while the active lattices hold fewer nodes than
+    that (enough work to fill the GPU; more only shares it and lengthens every solve).  With
+    nothing active, the first candidate is always admitted."""
+    if policy not in ("fifo", "sjf"):
+        raise ValueError(f"unknown admission policy {policy!r}")
+    order = arrived if policy == "fifo" else sorted(arrived, key=lambda r: (r.nodes * r.budget, r.arrival))
+    nodes = sum(r.nodes for r in active)
+    out = []
+    for r in order:
+        lone = not active and not out
+        need = footprint_bytes(r.case, precision)
+        if policy == "sjf" and max_active_nodes is not None and nodes >= max_active_nodes and not lone:
+            break
+        if used + need > hbm_budget and not lone:
+            if policy == "fifo":
+                break
+            continue
+        out.append(r)
+        used += need
+        nodes += r.nodes
+    return out
+
+
 def serve_batched(requests: list[Request], precision: str = "f16", device: int = 0, hbm_budget: float = 160e9,
                   chunk: int = 100, check_every: int = 500, clock=time.perf_counter, keep_results: bool = False,
-                  variant: int | None = None) -> dict:
-    """Continuous batching: admit while memory allows, advance all admitted solves together
-    (`variant`: the batch kernel, hlbm_batch_tune)."""
+                  variant: int | None = None, policy: str = "fifo", max_active_nodes: int | None = None) -> dict:
+    """Continuous batching: admit (`admit`: policy and cap) while memory allows, advance all
+    admitted solves together (`variant`: the batch kernel, hlbm_batch_tune)."""
     pending = sorted(requests, key=lambda r: r.arrival)
     active: list[Request] = []
     finished: list[Request] = []
@@ -132,15 +162,13 @@ def serve_batched(requests: list[Request], precision: str = "f16", device: int =
     try:
         while pending or active:
             now = clock() - start
-            while pending and pending[0].arrival <= now:
-                need = footprint_bytes(pending[0].case, precision)
-                if used + need > hbm_budget and active:
-                    break  # wait for memory to free up (a lone request is always admitted)
-                r = pending.pop(0)
+            arrived = [r for r in pending if r.arrival <= now]
+            for r in admit(arrived, active, used, precision, hbm_budget, policy, max_active_nodes):
+                pending.remove(r)
                 r.lat = Lattice.from_case(r.case, precision, device)
                 batch.add(r.lat)
                 r.admitted = now
-                used += need
+                used += footprint_bytes(r.case, precision)
                 active.append(r)
             if not active:
                 time.sleep(max(0.0, pending[0].arrival - (clock() - start)))
@@ -169,6 +197,7 @@ def serve_batched(requests: list[Request], precision: str = "f16", device: int =
         batch.close()
     out = _stats(finished, clock() - start, precision, "continuous batching")
     out["batch_variant"] = 8 if variant is None else variant
+    out["policy"] = policy if max_active_nodes is None else f"{policy}, max {max_active_nodes} active nodes"
     return out
 
 
