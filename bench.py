@@ -325,7 +325,7 @@ def run_ours(a):
                 "algorithmic_bytes_per_node": alg_bytes_per_node, "kernel": f"hlbm::{kname} (MODE_FUSED)"}
         cpu = None
         if not a.no_cpu_baseline and world == 1:
-            cpu_steps = 10
+            cpu_steps = 160  # about 10 s of host work on 16 cores
             mlups_c, kind, cores, dt = cpu_reference_mlups(a.cpu_n, cpu_steps, 2, a.collision, a.tau)
             cpu = {"value": round(mlups_c, 3), "unit": "MLUPS", "cores": cores, "kind": kind,
                    "sample": f"couette {a.cpu_n}^3 {a.collision} tau={a.tau} FP64, {cpu_steps} steps "
