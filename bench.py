@@ -74,7 +74,9 @@ def parse_args():
     ap.add_argument("--policy", default="fifo", choices=["fifo", "sjf"], help="serve workload: admission order")
     ap.add_argument("--max-active-nodes", type=int, default=0,
                     help="serve workload, sjf: admit while the active lattices hold fewer nodes (0: no cap)")
-    ap.add_argument("--batch-variant", type=int, default=8, help="batch and serve workloads: hlbm_batch_tune variant")
+    ap.add_argument("--batch-variant", type=int, default=-1,
+                    help="batch workload: hlbm_batch_tune variant (-1: 8, 9 and 10, report the fastest); "
+                         "serve workload: the batch variant (-1: 10)")
     ap.add_argument("--member-steps", type=int, default=2000, help="batch workload: steps of every lattice")
     ap.add_argument("--alone-steps", type=int, default=200,
                     help="batch workload: steps per lattice of the one-at-a-time comparison")
@@ -375,6 +377,8 @@ def run_precision(a):
 
 
 def run_batch(a):
+    """The batch workload with each batch kernel (--batch-variant, or 8, 9 and 10 with -1); the
+    line's value is the fastest, the others are listed."""
     import torch
 
     from hippolbm_b200.batch import Batch
@@ -383,31 +387,37 @@ def run_batch(a):
 
     torch.cuda.set_device(0)
     cases = mixed_batch_cases(a.members, steps=a.member_steps)
-    lats = [Lattice.from_case(c, "f32") for c in cases]
-    nodes = sum(l.ncell for l in lats)
-    batch = Batch("f32")
-    batch.tune(a.batch_variant)
-    for l in lats:
-        batch.add(l)
-    stream = torch.cuda.ExternalStream(batch.stream_handle(), device=torch.device("cuda", 0))
-    batch.step(a.warmup)
-    torch.cuda.synchronize()
-    info0 = batch.info()
-    clocks = ClockSampler(0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    batch.step(a.member_steps - a.warmup)
-    e1.record(stream)
-    e1.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    timed = a.member_steps - a.warmup
-    info = batch.info()
-    mlups = nodes * timed / (ms * 1e-3) / 1e6
-    batch.close()
-    for l in lats:
-        l.close()
-    # the same lattices one at a time, each with its own launches (variant 0, no graph)
+    variants = [8, 9, 10] if a.batch_variant < 0 else [a.batch_variant]
+    runs = {}
+    for variant in variants:
+        lats = [Lattice.from_case(c, "f32") for c in cases]
+        nodes = sum(l.ncell for l in lats)
+        batch = Batch("f32")
+        batch.tune(variant)
+        for l in lats:
+            batch.add(l)
+        stream = torch.cuda.ExternalStream(batch.stream_handle(), device=torch.device("cuda", 0))
+        batch.step(a.warmup)
+        torch.cuda.synchronize()
+        info0 = batch.info()
+        clocks = ClockSampler(0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.step(a.member_steps - a.warmup)
+        e1.record(stream)
+        e1.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        timed = a.member_steps - a.warmup
+        info = batch.info()
+        runs[variant] = {"mlups": round(nodes * timed / (ms * 1e-3) / 1e6, 1), "ms_per_step": round(ms / timed, 4),
+                         "gpu_launches": info["launches"] - info0["launches"],
+                         "graph_replays": info["graph_replays"] - info0["graph_replays"], "clocks": clk}
+        batch.close()
+        for l in lats:
+            l.close()
+    best = max(runs, key=lambda v: runs[v]["mlups"])
+    # the same lattices one at a time, each with its own launches (its default kernel, no graph)
     alone_ms = 0.0
     for c in cases:
         with Lattice.from_case(c, "f32") as l:
@@ -423,14 +433,16 @@ def run_batch(a):
     kinds = {}
     for c in cases:
         kinds[c.name.split("_")[1]] = kinds.get(c.name.split("_")[1], 0) + 1
-    line = {"workload": "batch", "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": 1,
-            "steps": timed, "warmup": a.warmup, "ms_per_step": round(ms / timed, 4), "higher_is_better": True,
+    r = runs[best]
+    timed = a.member_steps - a.warmup
+    line = {"workload": "batch", "metric": "MLUPS", "value": r["mlups"], "unit": "MLUPS", "n_gpus": 1,
+            "steps": timed, "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"mixed_batch_{a.members}", "members": a.members, "nodes": nodes,
-                       "kinds": kinds, "seed": 20261203, "kernel_variant": a.batch_variant},
-            "one_at_a_time_mlups": round(alone, 1), "speedup_vs_one_at_a_time": round(mlups / alone, 2),
-            "gpu_launches": info["launches"] - info0["launches"], "graph_replays": info["graph_replays"] - info0["graph_replays"],
-            "clocks": clk}
+                       "kinds": kinds, "seed": 20261203, "kernel_variant": best},
+            "by_variant": {str(v): runs[v]["mlups"] for v in runs},
+            "one_at_a_time_mlups": round(alone, 1), "speedup_vs_one_at_a_time": round(r["mlups"] / alone, 2),
+            "gpu_launches": r["gpu_launches"], "graph_replays": r["graph_replays"], "clocks": r["clocks"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -441,7 +453,7 @@ def run_serve(a):
     lines = []
     for rate in [float(r) for r in a.rates.split(",")]:
         fast = serve.serve_batched(serve.make_stream(rate, a.requests), "f16", hbm_budget=160e9,
-                                   variant=a.batch_variant, policy=a.policy,
+                                   variant=a.batch_variant if a.batch_variant >= 0 else 10, policy=a.policy,
                                    max_active_nodes=a.max_active_nodes or None)
         plain = serve.serve_plain(serve.make_stream(rate, a.requests), "f64")
         lines.append({"rate": rate, "batched_f16": fast, "plain_f64": plain,
