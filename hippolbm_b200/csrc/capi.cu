@@ -402,6 +402,9 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   c->launches++;
   if (face_pass_runs(p, walls, variant, mode == MODE_PROLOGUE, int(elem_size(c->precision))))
     c->launches++;  // the face pass after the step kernel
+  if (walls && mode != MODE_PROLOGUE && variant < 6 && variant % 2 == 1 &&
+      vec_eligible_bytes(p, walls, int(elem_size(c->precision))))
+    c->launches++;  // the wall fix-up after the vectorised kernel
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
     case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, s, variant, t);
@@ -434,8 +437,7 @@ cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fou
 
 // the vectorised kernel applies (launch.cuh: vec_eligible)
 bool vec_applies(const hlbm_ctx* c) {
-  const int npt = elem_size(c->precision) == 2 ? 4 : 2;
-  return !c->plan.walls && c->n[0] % npt == 0 && c->n[0] / npt >= 32;
+  return vec_eligible_bytes(c->plan, c->plan.walls, int(elem_size(c->precision)));
 }
 
 // make S_k available; returns the buffer holding it

@@ -84,11 +84,12 @@ struct StepPlan {
 
 // Nodes per thread of the vectorised step kernel for a storage type of `bytes` bytes (one 8-byte
 // vector per direction plane for 2- and 4-byte types, double2 for FP64), and whether a lattice
-// can use it: no wall obstacles, whole vectors per row and at least one warp of them.
+// can use it: whole vectors per row and at least one warp of them.
 inline constexpr int vec_npt_bytes(int bytes) { return bytes == 2 ? 4 : 2; }
 inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes) {
+  (void)walls;  // wall obstacles: the wall fix-up pass follows the vectorised kernel
   const int npt = vec_npt_bytes(bytes);
-  return !walls && p.nx % npt == 0 && p.nx / npt >= 32;
+  return p.nx % npt == 0 && p.nx / npt >= 32;
 }
 
 // Whether the 16-bit one-node kernel can run two nodes per thread: even z-planes (every pair on a

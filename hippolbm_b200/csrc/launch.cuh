@@ -102,7 +102,8 @@ inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, di
 }
 
 template <typename S, typename R, bool STRICT, int MODE, int MINB>
-cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const StepPlan& p, cudaStream_t s) {
+cudaError_t launch_vec(int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                       cudaStream_t s) {
   constexpr int NPT = vec_npt<S>();
   dim3 grid, block;
   vec_geometry(p, NPT, 0, grid, block);
@@ -115,7 +116,16 @@ cudaError_t launch_vec(const void* fin, void* fout, const int8_t* flags, const S
   else
     k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
   if (cudaError_t e = cudaGetLastError()) return e;
-  return launch_faces<S, R, STRICT, MODE, false>(fi, fo, flags, p, s);
+  if (cudaError_t e = launch_faces<S, R, STRICT, MODE, false>(fi, fo, flags, p, s)) return e;
+  if (!walls || MODE == MODE_PROLOGUE) return cudaSuccess;
+  const unsigned wgrid = unsigned((p.ncell + 255) / 256);
+  if (MODE == MODE_FUSED && p.collision == 0)
+    k_wall_fixup<S, R, STRICT, MODE, 0><<<wgrid, 256, 0, s>>>(fi, fo, flags, p);
+  else if (MODE == MODE_FUSED)
+    k_wall_fixup<S, R, STRICT, MODE, 1><<<wgrid, 256, 0, s>>>(fi, fo, flags, p);
+  else
+    k_wall_fixup<S, R, STRICT, MODE, 2><<<wgrid, 256, 0, s>>>(fi, fo, flags, p);
+  return cudaGetLastError();
 }
 
 // Step kernel variants 0..5: variant % 2 selects the kernel (0: one node per thread, 1:
@@ -173,9 +183,9 @@ template <typename S, typename R, bool STRICT, int MINB>
 cudaError_t launch_minb(int mode, int walls, bool vec, const void* fin, void* fout, const int8_t* flags,
                         const StepPlan& p, cudaStream_t s) {
   if (vec) {
-    if (mode == MODE_PROLOGUE) return launch_vec<S, R, STRICT, MODE_PROLOGUE, MINB>(fin, fout, flags, p, s);
-    if (mode == MODE_FUSED) return launch_vec<S, R, STRICT, MODE_FUSED, MINB>(fin, fout, flags, p, s);
-    return launch_vec<S, R, STRICT, MODE_FINISH, MINB>(fin, fout, flags, p, s);
+    if (mode == MODE_PROLOGUE) return launch_vec<S, R, STRICT, MODE_PROLOGUE, MINB>(walls, fin, fout, flags, p, s);
+    if (mode == MODE_FUSED) return launch_vec<S, R, STRICT, MODE_FUSED, MINB>(walls, fin, fout, flags, p, s);
+    return launch_vec<S, R, STRICT, MODE_FINISH, MINB>(walls, fin, fout, flags, p, s);
   }
   if (mode == MODE_PROLOGUE)
     return walls ? launch_one<S, R, STRICT, MODE_PROLOGUE, true, MINB>(fin, fout, flags, p, s)

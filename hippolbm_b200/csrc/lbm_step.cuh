@@ -1066,4 +1066,22 @@ __global__ void __launch_bounds__(256) k_faces(const S* __restrict__ fin, S* __r
   node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
 }
 
+// The wall fix-up after the vectorised kernel, which pulls without testing for wall nodes: every
+// node the near-wall map marks (some pull may come from a wall) is stepped again by the one-node
+// step with the wall test, and a read-out gives wall nodes the read-out value of a wall.  It runs
+// after the face pass and reads only fin, so its result replaces both.
+template <typename S, typename R, bool STRICT, int MODE, int COLL>
+__global__ void __launch_bounds__(256) k_wall_fixup(const S* __restrict__ fin, S* __restrict__ fout,
+                                                    const int8_t* __restrict__ flags, const StepPlan p) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= p.ncell) return;
+  const bool near = p.nearwall == nullptr || p.nearwall[idx] != 0;
+  if (!near && !(MODE == MODE_FINISH && flags[idx] == FLAG_WALL)) return;
+  const int64_t plane = int64_t(p.nx) * p.ny;
+  const int z = int(idx / plane);
+  const int64_t r = idx - int64_t(z) * plane;
+  const int y = int(r / p.nx), x = int(r - int64_t(y) * p.nx);
+  node_step<S, R, STRICT, MODE, true, COLL>(fin, fout, flags, p, x, y, z);
+}
+
 }  // namespace hlbm
