@@ -195,9 +195,9 @@ int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
 /* info = {nx, ny, nz, precision, steps done, kernel launches, bytes per population, device} */
 int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
 /* Step kernel selection (no reference counterpart).  Variants 0..5: variant % 2 picks the kernel,
- * 0 = one node per thread, 1 = vectorised (consecutive x-nodes per thread in one vector per
- * direction plane; used when the lattice has no wall obstacles and nx splits into >= 32 vectors,
- * else the first kernel runs); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256
+ * 0 = one node per thread (two per thread for the 16-bit tiers), 1 = vectorised (consecutive
+ * x-nodes per thread in one vector per direction plane; used when nx splits into >= 32 vectors,
+ * else the first kernel runs; with wall obstacles a fix-up pass re-steps the nodes next to walls); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256
  * threads per SM.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
  * into shared-memory stages (256 or 512 threads per CTA; needs nx * bytes per population to be a
  * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
