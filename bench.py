@@ -40,7 +40,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_POP = {"f64": 8, "f64_strict": 8, "f32": 4, "f16": 2, "bf16": 2}
-DEFAULT_VARIANT = {"f64": 4, "f64_strict": 4, "f32": 5, "f16": 5, "bf16": 5}
+DEFAULT_VARIANT = {("f64", "bgk"): 4, ("f64", "mrt"): 4, ("f64_strict", "bgk"): 4, ("f64_strict", "mrt"): 4,
+                   ("f32", "bgk"): 1, ("f32", "mrt"): 1, ("f16", "bgk"): 5, ("f16", "mrt"): 3,
+                   ("bf16", "bgk"): 5, ("bf16", "mrt"): 3}
 DTYPE = {"f64": "f64", "f64_strict": "f64", "f32": "f32", "f16": "f32 (f16 storage)", "bf16": "f32 (bf16 storage)"}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -61,7 +63,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=128, help="lattice edge of the CPU baseline sample")
     ap.add_argument("--variant", type=int, default=-1,
-                    help="step-kernel variant; -1: the tier's default (4 for FP64, 5 for FP32 and 16-bit)")
+                    help="step-kernel variant; -1: the tier's default (the autotuner's pick on 512^3 Couette)")
     ap.add_argument("--autotune", action="store_true", help="time every variant on the lattice and keep the fastest")
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="16-bit storage rounding")
@@ -253,7 +255,7 @@ def run_ours(a):
     if a.autotune:
         variant, variant_ms = lat.autotune(reps=3)
     else:
-        variant, variant_ms = (a.variant if a.variant >= 0 else DEFAULT_VARIANT[a.precision]), {}
+        variant, variant_ms = (a.variant if a.variant >= 0 else DEFAULT_VARIANT[(a.precision, a.collision)]), {}
         lat.tune(variant)
     # warm-up
     lat.step(a.warmup)

@@ -124,6 +124,8 @@ struct hlbm_ctx {
   int cur = 0;
   int8_t* flags = nullptr;
   int8_t* nearwall = nullptr;  // per node: some pull comes from a wall node (k_near_wall)
+  bool maybe_walls = false;     // the flags may hold wall nodes (an obstacle was rasterised or put)
+  bool variant_tuned = false;   // hlbm_tune / hlbm_autotune chose the variant (else the tier default)
   double* partials = nullptr;
   double* stats_dev = nullptr;
   double* plane_tmp = nullptr;
@@ -206,6 +208,7 @@ void base_plan(hlbm_ctx* c, StepPlan& p) {
   p.stride = c->stride;
   p.rho0 = c->rho0;
   p.nearwall = c->nearwall;
+  p.wall_flags = c->maybe_walls ? 1 : 0;
   p.scale = c->scale;
   p.inv_scale = 1.0 / c->scale;
   storage_reference(c, p.dref);
@@ -299,6 +302,10 @@ int build_plan(hlbm_ctx* c) {
   p.inv_tau = 1.0 / c->tau;
   for (int d = 0; d < 3; d++) p.F[d] = c->Fext[d];
   p.has_force = (c->Fext[0] != 0.0 || c->Fext[1] != 0.0 || c->Fext[2] != 0.0) ? 1 : 0;
+  for (int i = 0; i < Q; i++) {
+    p.fw3[i] = 3. * W_OF(i) * (D3Q19::ex[i] * c->Fext[0] + D3Q19::ey[i] * c->Fext[1] + D3Q19::ez[i] * c->Fext[2]);
+    p.ffw3[i] = float(p.fw3[i]);
+  }
   for (int k = 0; k < 8; k++) p.mrt[k] = c->mrt[k];
   bool pre_seen = false;
   for (const HookOp& h : c->hooks) {
@@ -403,7 +410,7 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   if (face_pass_runs(p, walls, variant, mode == MODE_PROLOGUE, int(elem_size(c->precision))))
     c->launches++;  // the face pass after the step kernel
   if (walls && mode != MODE_PROLOGUE && variant < 6 && variant % 2 == 1 &&
-      vec_eligible_bytes(p, walls, int(elem_size(c->precision))))
+      vec_eligible_bytes(p, walls, int(elem_size(c->precision)), variant))
     c->launches++;  // the wall fix-up after the vectorised kernel
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
@@ -435,9 +442,9 @@ cudaError_t launch_step_kernel(hlbm_ctx* c, int mode, const void* fin, void* fou
   return launch_step_variant(c, mode, fin, fout, c->variant);
 }
 
-// the vectorised kernel applies (launch.cuh: vec_eligible)
-bool vec_applies(const hlbm_ctx* c) {
-  return vec_eligible_bytes(c->plan, c->plan.walls, int(elem_size(c->precision)));
+// the vectorised kernel of `variant` applies (d3q19.cuh: vec_eligible_bytes)
+bool vec_applies(const hlbm_ctx* c, int variant) {
+  return vec_eligible_bytes(c->plan, c->plan.walls, int(elem_size(c->precision)), variant);
 }
 
 // make S_k available; returns the buffer holding it
@@ -485,6 +492,15 @@ extern "C" {
 const char* hlbm_last_error(void) { return g_err.c_str(); }
 const char* hlbm_version(void) { return "hippolbm-b200 0.1.0 (sm_100a)"; }
 
+// Default step-kernel variant of a tier and collision: hlbm_autotune's pick on 512^3 Couette on a
+// B200.  FP64: one node per thread at >= 3 blocks/SM (4); FP32: 16-byte vectors at one block/SM
+// (1); FP16 / BF16: 8-byte vectors at >= 3 blocks/SM (5) for BGK, >= 2 blocks/SM (3) for MRT.
+static int default_variant(int precision, int collision) {
+  if (precision == HLBM_F64 || precision == HLBM_F64_STRICT) return 4;
+  if (precision == HLBM_F32) return 1;
+  return collision == 1 ? 3 : 5;
+}
+
 int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],
                 int32_t precision, int32_t device, hlbm_ctx** out) {
   if (!cell_dims || !bmin || !bmax || !periodic || !out) return fail(HLBM_EINVAL, "hlbm_domain: NULL argument");
@@ -514,9 +530,7 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
   c->ncell = int64_t(n[0]) * n[1] * n[2];
   c->stride = (c->ncell + 127) / 128 * 128;
   if (precision == HLBM_F16) c->scale = 1024.0;
-  // default step-kernel variant per tier, from hlbm_autotune on 512^3 Couette (B200): FP64 one
-  // node per thread at >= 3 blocks/SM; FP32, FP16 and BF16 vectorised at >= 3 blocks/SM
-  c->variant = (precision == HLBM_F64 || precision == HLBM_F64_STRICT) ? 4 : 5;
+  c->variant = default_variant(precision, 0);
   mrt_reference(c->mrt);
   auto cleanup = [&](int rc) {
     hlbm_destroy(c);
@@ -638,6 +652,7 @@ int hlbm_collision(hlbm_ctx* c, int32_t kind, const double* rates8) {
   StepPlan old_plan;
   base_plan(c, old_plan);
   c->collision = kind;
+  if (!c->variant_tuned) c->variant = default_variant(c->precision, kind);
   if (rates8)
     std::memcpy(c->mrt, rates8, sizeof(c->mrt));
   else
@@ -767,8 +782,17 @@ int hlbm_update_obstacles(hlbm_ctx* c) {
     if (!clip_box(c, mn, mx, lo, hi)) continue;
     c->launches++;
     HLBM_CK(launch_rasterize(c->flags, p, lo, hi, c->dx, o, c->stream));
+    c->maybe_walls = true;
+    c->plan_dirty = true;
   }
   return refresh_near_wall(c);
+}
+
+// whether a host flag array holds a wall node
+static bool any_wall(const int8_t* flags, int64_t n) {
+  for (int64_t i = 0; i < n; i++)
+    if (flags[i] == FLAG_WALL) return true;
+  return false;
 }
 
 int hlbm_clear_hooks(hlbm_ctx* c) {
@@ -1015,6 +1039,8 @@ int hlbm_put_flags(hlbm_ctx* c, const int8_t* in) {
   if (int rc = set_device(c)) return rc;
   HLBM_CK(cudaMemcpyAsync(c->flags, in, size_t(c->ncell), cudaMemcpyHostToDevice, c->stream));
   if (int rc = refresh_near_wall(c)) return rc;
+  c->maybe_walls = any_wall(in, c->ncell);
+  c->plan_dirty = true;
   HLBM_CK(cudaStreamSynchronize(c->stream));
   return HLBM_OK;
 }
@@ -1120,6 +1146,7 @@ int hlbm_checkpoint_load(hlbm_ctx* c, const void* host, int64_t bytes) {
   const size_t n = size_t(c->ncell), es = elem_size(c->precision);
   HLBM_CK(cudaMemcpyAsync(c->flags, in, n, cudaMemcpyHostToDevice, c->stream));
   if (int rc = refresh_near_wall(c)) return rc;
+  c->maybe_walls = any_wall(reinterpret_cast<const int8_t*>(in), int64_t(n));
   in += n;
   HLBM_CK(cudaMemcpy2DAsync(c->f[c->cur], size_t(c->stride) * es, in, n * es, n * es, Q, cudaMemcpyHostToDevice,
                             c->stream));
@@ -1150,6 +1177,7 @@ int hlbm_tune(hlbm_ctx* c, int32_t variant) {
   if (!c || variant < 0 || variant >= NUM_VARIANTS)
     return fail(HLBM_EINVAL, "hlbm_tune: variant must be in [0, " + std::to_string(NUM_VARIANTS) + ")");
   c->variant = variant;
+  c->variant_tuned = true;
   return HLBM_OK;
 }
 
@@ -1168,7 +1196,7 @@ int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_var
   float best_ms = 1e30f;
   for (int v = 0; v < NUM_VARIANTS; v++) {
     if (ms_per_variant) ms_per_variant[v] = -1.0;
-    if (v < 6 && (v % 2) == 1 && !vec_applies(c)) continue;
+    if (v < 6 && (v % 2) == 1 && !vec_applies(c, v)) continue;
     if (v >= 6 && c->tma_stages < 2) continue;
     cudaError_t e = launch_step_variant(c, MODE_FUSED, fin, fout, v);  // warm-up
     if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
@@ -1193,6 +1221,7 @@ int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_var
   cudaEventDestroy(e1);
   if (int rc = check_device_error(c)) return rc;
   c->variant = best;
+  c->variant_tuned = true;
   if (chosen) *chosen = best;
   return HLBM_OK;
 }

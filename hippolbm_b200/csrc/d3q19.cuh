@@ -58,6 +58,8 @@ struct StepPlan {
   int32_t ncav[6];    // cavity coefficient sets per face (z faces only)
   double tau, inv_tau;
   double F[3];
+  double fw3[Q];      // 3 w_i (e_i . F): the force term of a collision is fw3_i * rho
+  float ffw3[Q];      // the same in FP32
   double mrt[8];      // s_e, s_eps, s_q, s_pi, s_m, w_eps, w_epsj, w_xx
   double cav[6][MAX_CAVITY][5];
   double rho0;        // reference density of the deviation storage
@@ -78,25 +80,42 @@ struct StepPlan {
   // per node: 1 when some direction pulls from a wall node (k_near_wall); nodes with 0 skip the
   // wall test of every pull.  Null: test every pull.
   const int8_t* nearwall;
+  // the flags may hold wall nodes (an obstacle was rasterised or wall flags were put)
+  int32_t wall_flags;
   PlaneOp ops[MAX_PLANE_OPS];
   SetBox sets[MAX_SETS];
 };
 
-// Nodes per thread of the vectorised step kernel for a storage type of `bytes` bytes (one 8-byte
-// vector per direction plane for 2- and 4-byte types, double2 for FP64), and whether a lattice
-// can use it: whole vectors per row and at least one warp of them.
-inline constexpr int vec_npt_bytes(int bytes) { return bytes == 2 ? 4 : 2; }
-inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes) {
+// Whether the kernels that update node pairs in packed FP32 (the vectorised kernel of the 4- and
+// 2-byte tiers, the 16-bit pair kernel) take a plan: no start_iteration boxes, no body force (the
+// force term would hold the pair's density in registers through the whole update), and wall nodes
+// only where wall_bounce_back makes their populations scratch (a pair collides both lanes).  Other
+// plans run the one-node kernel.
+inline bool pair_kernels_apply(const StepPlan& p, int bytes) {
+  return bytes == 8 || (p.nsets == 0 && !p.has_force && (!p.wall_flags || p.walls));
+}
+
+// Nodes per thread of the vectorised step kernel for a storage type of `bytes` bytes: one 16-byte
+// vector per direction plane (double2; float4 and 8 packed 16-bit values at the lowest occupancy
+// target, 1 CTA of 256 threads per SM, up to 255 registers), or one 8-byte vector for the 4- and
+// 2-byte types at the higher targets (128 / 80 registers); and whether a lattice can use it:
+// whole vectors per row, at least one warp of them, node offsets that fit 32 bits, and the
+// conditions of pair_kernels_apply.
+inline constexpr int vec_npt_bytes(int bytes, int minb) {
+  return bytes == 8 ? 2 : (minb <= 1 ? 16 : 8) / bytes;
+}
+inline constexpr int variant_minb(int variant) { return variant / 2 + 1; }
+inline bool vec_eligible_bytes(const StepPlan& p, int walls, int bytes, int variant) {
   (void)walls;  // wall obstacles: the wall fix-up pass follows the vectorised kernel
-  const int npt = vec_npt_bytes(bytes);
-  return p.nx % npt == 0 && p.nx / npt >= 32;
+  const int npt = vec_npt_bytes(bytes, variant_minb(variant));
+  return p.nx % npt == 0 && p.nx / npt >= 32 && p.ncell <= int64_t(0xffffffffu) && pair_kernels_apply(p, bytes);
 }
 
 // Whether the 16-bit one-node kernel can run two nodes per thread: even z-planes (every pair on a
-// 4-byte boundary) of fewer than 2^24 nodes.
+// 4-byte boundary) of fewer than 2^24 nodes, and pair_kernels_apply.
 inline bool pairs_eligible(const StepPlan& p) {
   const int64_t plane = int64_t(p.nx) * p.ny;
-  return plane % 2 == 0 && plane < (int64_t(1) << 24);
+  return plane % 2 == 0 && plane < (int64_t(1) << 24) && pair_kernels_apply(p, 2);
 }
 
 // Whether a single-lattice launch of step variant `variant` (not the prologue) is followed by the
@@ -104,7 +123,7 @@ inline bool pairs_eligible(const StepPlan& p) {
 // pipelined kernel (variants 6, 7) applies the operators inline.
 inline bool face_pass_runs(const StepPlan& p, int walls, int variant, bool prologue, int bytes) {
   if (variant >= 6 || prologue || p.face_mask == 0) return false;
-  return (variant % 2 == 1 && vec_eligible_bytes(p, walls, bytes)) || bytes < 8;
+  return (variant % 2 == 1 && vec_eligible_bytes(p, walls, bytes, variant)) || bytes < 8;
 }
 
 // Faces whose nodes the boundary operators of the plan can change: every non-periodic face for

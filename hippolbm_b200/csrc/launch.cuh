@@ -79,16 +79,10 @@ cudaError_t launch_one(const void* fin, void* fout, const int8_t* flags, const S
   return cudaSuccess;
 }
 
-// nodes per thread of the vectorised kernel: one 8-byte vector per direction plane for the
-// 4- and 2-byte storage types (float2, 4 x FP16/BF16); FP64 uses double2
-template <typename S>
+// nodes per thread of the vectorised kernel at occupancy target MINB (d3q19.cuh: vec_npt_bytes)
+template <typename S, int MINB>
 constexpr int vec_npt() {
-  return vec_npt_bytes(int(sizeof(S)));
-}
-
-template <typename S>
-bool vec_eligible(const StepPlan& p, int walls) {
-  return vec_eligible_bytes(p, walls, int(sizeof(S)));
+  return vec_npt_bytes(int(sizeof(S)), MINB);
 }
 
 inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, dim3& block) {
@@ -104,17 +98,18 @@ inline void vec_geometry(const StepPlan& p, int npt, int block_x, dim3& grid, di
 template <typename S, typename R, bool STRICT, int MODE, int MINB>
 cudaError_t launch_vec(int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
                        cudaStream_t s) {
-  constexpr int NPT = vec_npt<S>();
+  constexpr int NPT = vec_npt<S, MINB>();
   dim3 grid, block;
   vec_geometry(p, NPT, 0, grid, block);
   const S* fi = static_cast<const S*>(fin);
   S* fo = static_cast<S*>(fout);
+  const Planes<S> pl = make_planes(fi, fo, p.stride);
   if (MODE == MODE_FUSED && p.collision == 0)
-    k_step_vec<S, R, STRICT, MODE, NPT, 0, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+    k_step_vec<S, R, STRICT, MODE, NPT, 0, MINB><<<grid, block, 0, s>>>(pl, flags, p);
   else if (MODE == MODE_FUSED)
-    k_step_vec<S, R, STRICT, MODE, NPT, 1, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+    k_step_vec<S, R, STRICT, MODE, NPT, 1, MINB><<<grid, block, 0, s>>>(pl, flags, p);
   else
-    k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(fi, fo, flags, p);
+    k_step_vec<S, R, STRICT, MODE, NPT, 2, MINB><<<grid, block, 0, s>>>(pl, flags, p);
   if (cudaError_t e = cudaGetLastError()) return e;
   if (cudaError_t e = launch_faces<S, R, STRICT, MODE, false>(fi, fo, flags, p, s)) return e;
   if (!walls || MODE == MODE_PROLOGUE) return cudaSuccess;
@@ -233,7 +228,7 @@ cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const 
     if (mode == MODE_FUSED && tma.stages >= 2) return launch_tma<S, R, STRICT>(tma, walls, tma.ctas_per_sm, s);
     variant = 4;
   }
-  const bool vec = (variant % 2) == 1 && vec_eligible<S>(p, walls);
+  const bool vec = (variant % 2) == 1 && vec_eligible_bytes(p, walls, int(sizeof(S)), variant);
   if ((variant % 2) == 1 && !vec) variant = 4;  // no vectorised kernel for this lattice: 3 CTAs/SM scalar
   switch (variant / 2) {
     case 0: return launch_minb<S, R, STRICT, 1>(mode, walls, vec, fin, fout, flags, p, s);

@@ -23,7 +23,10 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "d3q19.cuh"
+#include "lanes.cuh"
 
 namespace hlbm {
 
@@ -225,24 +228,6 @@ __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, u
   }
 }
 
-// Stores the Q values of two x-neighbours a (node idx, low half) and b (node idx + 1, high half)
-// of a 16-bit tier as packed pairs dst(I, word): one conversion per direction and pair, the
-// random bits hashed from the pair's first node.
-template <typename S, typename R, int MODE, class Dst>
-__device__ __forceinline__ void store_pair(const R (&a)[Q], const R (&b)[Q], const StepPlan& p, uint32_t seed,
-                                           int64_t idx, Dst&& dst) {
-  static_assert(is_16bit<S>(), "packed pairs are 16-bit storage");
-  if (MODE != MODE_FINISH && p.rounding) {
-    const uint32_t h = node_hash(idx, seed);
-    const uint32_t h2 = second_hash(h);
-    Unroll<0, Q>::run([&]<int I>() {
-      dst.template operator()<I>(Codec<S, R>::template encd_sr2<I>(a[I], b[I], pair_bits<I>(h, h2)));
-    });
-  } else {
-    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd2<I>(a[I], b[I])); });
-  }
-}
-
 // The launch's step number (the stochastic-rounding salt): from the plan, or from the device
 // counter pair of a graph-replayed launch (see StepPlan::seed_dev).
 template <typename S>
@@ -274,6 +259,27 @@ __device__ __forceinline__ R load_value(S raw, const StepPlan& p) {
 template <typename R, int I>
 __device__ __forceinline__ constexpr R weight() {
   return R(1.0) / R(D3Q19::wden[I]);
+}
+
+// The read-out value of a wall node (population 0) as the kernels carry it: 0, or for the 16-bit
+// tiers the scaled deviation -dref_I * scale.
+template <typename S, int I>
+__device__ __forceinline__ float wall_value(const StepPlan& p) {
+  if constexpr (is_16bit<S>())
+    return -p.dref[I] * float(p.scale);
+  else
+    return 0.0f;
+}
+
+// The value a start_iteration set_distribution box writes into direction I (f_i = value * w_i,
+// set_distribution.hpp:29-46), as the kernels carry it: full populations, or for the 16-bit tiers
+// the scaled deviation from the storage reference.
+template <typename S, typename R, int I>
+__device__ __forceinline__ R set_value(double value, const StepPlan& p) {
+  if constexpr (is_16bit<S>())
+    return (__fmul_rn(R(value), weight<R, I>()) - R(p.dref[I])) * R(p.scale);
+  else
+    return R(value) * weight<R, I>();
 }
 
 // sum_{axis} e_axis * a_axis over the non-zero components in x, y, z order: the value of the
@@ -496,112 +502,170 @@ __device__ __forceinline__ void mrt(R (&v)[Q], const StepPlan& p) {
 constexpr bool mrt_even(int k) { return k <= 2 || (k >= 9 && k <= 15); }
 constexpr bool mrt_conserved(int k) { return k == 0 || k == 3 || k == 5 || k == 7; }
 
-template <typename R>
-__device__ __forceinline__ R fmar(R a, R b, R c) {
-  if constexpr (sizeof(R) == 4)
-    return fmaf(a, b, c);
-  else
-    return fma(a, b, c);
+// e_I . a for an odd direction I, whose first non-zero component is +1 (1, 3, 5, 7, 9, 11, 13,
+// 15, 17): in x, y, z order with no negation.  Its opposite I + 1 has e . a = -(this) exactly.
+template <int I, typename V>
+__device__ __forceinline__ V edot_odd(V ax, V ay, V az) {
+  using L = Lanes<V>;
+  static_assert(I & 1, "odd directions only");
+  constexpr int cx = D3Q19::ex[I], cy = D3Q19::ey[I], cz = D3Q19::ez[I];
+  if constexpr (cx != 0) {
+    static_assert(cx == 1, "first component +1");
+    V acc = ax;
+    if constexpr (cy != 0) acc = cy > 0 ? L::add(acc, ay) : L::sub(acc, ay);
+    if constexpr (cz != 0) acc = cz > 0 ? L::add(acc, az) : L::sub(acc, az);
+    return acc;
+  } else if constexpr (cy != 0) {
+    static_assert(cy == 1, "first component +1");
+    V acc = ay;
+    if constexpr (cz != 0) acc = cz > 0 ? L::add(acc, az) : L::sub(acc, az);
+    return acc;
+  } else {
+    return az;
+  }
 }
 
-// The same MRT collision for the FMA tiers, in fewer operations.  Directions 2p-1 and 2p are
-// opposites, so an even moment sums S_p = f_{2p-1} + f_{2p} and an odd one D_p = f_{2p-1} - f_{2p}
-// (about half the terms of the full transform), and the back-transform (the exact inverse of the
-// basis) gives each opposite pair from one even part E_p and one odd part O_p as E_p +- O_p.  Only
-// the non-conserved moments change, so the update is f_i -= sum_k Minv[i][k] dm_k with
-// dm_k = m_k - m_k*, the relaxation of moment k.  Same equilibria and rates as `mrt`; the
-// operation order differs, so results agree with it to rounding.
-template <typename R, bool DEVF>
-__device__ __forceinline__ void mrt_fast(R (&v)[Q], const StepPlan& p) {
-  R S[10], D[10];
-  Unroll<1, 10>::run([&]<int P>() {
-    S[P] = v[2 * P - 1] + v[2 * P];
-    D[P] = v[2 * P - 1] - v[2 * P];
-  });
-  R m[19];
-  Unroll<0, 19>::run([&]<int K>() {
-    constexpr bool EV = mrt_even(K);
-    R acc = R(0);
-    bool first = true;
-    if constexpr (EV) {
-      constexpr int c0 = MrtTables::M[K][0];
-      if constexpr (c0 != 0) {
-        acc = c0 == 1 ? v[0] : R(c0) * v[0];
-        first = false;
-      }
-    }
-    Unroll<1, 10>::run([&]<int P>() {
-      constexpr int c = MrtTables::M[K][2 * P - 1];
-      if constexpr (c != 0) {
-        const R x = EV ? S[P] : D[P];
-        if (first)
-          acc = c == 1 ? x : (c == -1 ? -x : R(c) * x);
-        else
-          acc = c == 1 ? acc + x : (c == -1 ? acc - x : fmar(R(c), x, acc));
-        first = false;
-      }
+// ------------------------------------------------------------------ packed 16-bit node pairs
+// The two 16-bit values of a packed word as FP32 lanes (low half-word in .x).
+template <typename S>
+__device__ __forceinline__ float2 unpack2(uint32_t w) {
+  if constexpr (sizeof(S) == 2 && std::is_same_v<S, __half>) {
+    return __half22float2(*reinterpret_cast<const __half2*>(&w));
+  } else {
+    return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+  }
+}
+
+// A node pair of a 16-bit tier in FP32 lanes, rounded into one packed word per direction: with
+// stochastic rounding (sr) from the random bits pair_bits(h, h2) of the pair's first node, else to
+// nearest.  dst(I, word) stores direction I.
+template <typename S, class Dst>
+__device__ __forceinline__ void pack_pair(const float2 (&v)[Q], bool sr, uint32_t h, uint32_t h2, Dst&& dst) {
+  if (sr)
+    Unroll<0, Q>::run([&]<int I>() {
+      dst.template operator()<I>(Codec<S, float>::template encd_sr2<I>(v[I].x, v[I].y, pair_bits<I>(h, h2)));
     });
-    m[K] = acc;
+  else
+    Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, float>::template encd2<I>(v[I].x, v[I].y)); });
+}
+
+// ------------------------------------------------------------------ MRT, FMA tiers
+// S_p = f_{2p-1} + f_{2p} and D_p = f_{2p-1} - f_{2p} for the nine opposite pairs p = 1..9.  The
+// first pair with a non-zero coefficient in moment row K (0: the rest direction).
+template <int K>
+constexpr int mrt_first_term() {
+  constexpr bool EV = mrt_even(K);
+  if (EV && MrtTables::M[K][0] != 0) return 0;
+  for (int P = 1; P < 10; P++)
+    if (MrtTables::M[K][2 * P - 1] != 0) return P;
+  return 10;
+}
+
+// The MRT collision of every tier except strict FP64, in about half the reference's operations.
+// Directions 2p-1 and 2p are opposites, so an even moment sums S_p and an odd one D_p (about half
+// the terms of the full transform), and the back-transform (the exact inverse of the basis) gives
+// each opposite pair from one even and one odd part E_p, O_p as E_p +- O_p.  Only the
+// non-conserved moments change, so the update is f_i -= sum_k Minv[i][k] dm_k with
+// dm_k = m_k - m_k*, the relaxation of moment k.  Same equilibria and rates as `mrt`; the
+// operation order differs, so results agree with it to rounding.  V is one node (float, double)
+// or a node pair (float2); every operation is explicit (Lanes), so the pair form rounds as the
+// one-node form on each lane.
+// DEVF: v holds scaled deviations from the storage reference (the MRT rest state, whose moments
+// are rho0, e = -11 rho0, eps = w_eps rho0 and zero otherwise).  The moments of v are then the
+// scaled deviations of the moments, the e / eps equilibria take the density deviation m[0], the
+// quadratic equilibrium terms take one factor 1/scale, and the force term the full density.
+template <typename V, bool DEVF>
+__device__ __forceinline__ void mrt_fast(V (&v)[Q], const StepPlan& p) {
+  using L = Lanes<V>;
+  using T = typename L::S;
+  // moments in each row's term order, from the pair parts S_p, D_p
+  V m[19];
+  auto term = [&]<int K, int P>(V x) {
+    constexpr int c = P == 0 ? MrtTables::M[K][0] : MrtTables::M[K][2 * P - 1];
+    if constexpr (c != 0) {
+      if constexpr (mrt_first_term<K>() == P)
+        m[K] = c == 1 ? x : L::mul(L::splat(T(c)), x);
+      else
+        m[K] = c == 1 ? L::add(m[K], x) : (c == -1 ? L::sub(m[K], x) : L::fma(L::splat(T(c)), x, m[K]));
+    }
+  };
+  Unroll<0, 19>::run([&]<int K>() {
+    if constexpr (mrt_even(K)) term.template operator()<K, 0>(v[0]);
   });
-  const R rho = m[0], e = m[1], eps = m[2], jx = m[3], qx = m[4], jy = m[5], qy = m[6], jz = m[7], qz = m[8],
+  {
+    V S[10], D[10];
+    Unroll<1, 10>::run([&]<int P>() {
+      S[P] = L::add(v[2 * P - 1], v[2 * P]);
+      D[P] = L::sub(v[2 * P - 1], v[2 * P]);
+    });
+    Unroll<0, 19>::run([&]<int K>() {
+      Unroll<1, 10>::run([&]<int P>() { term.template operator()<K, P>(mrt_even(K) ? S[P] : D[P]); });
+    });
+  }
+  const V rho = m[0], e = m[1], eps = m[2], jx = m[3], qx = m[4], jy = m[5], qy = m[6], jz = m[7], qz = m[8],
           pxx3 = m[9], pixx3 = m[10], pww = m[11], piww = m[12], pxy = m[13], pyz = m[14], pxz = m[15];
-  const R s9 = R(p.inv_tau), s13 = s9;
-  const R s1 = R(p.mrt[0]), s2 = R(p.mrt[1]), s4 = R(p.mrt[2]), s10 = R(p.mrt[3]), s16 = R(p.mrt[4]);
-  const R weps = R(p.mrt[5]), wepsj = R(p.mrt[6]), wxx = R(p.mrt[7]);
-  const R qs = DEVF ? R(p.inv_scale) : R(1);
-  const R jxq = DEVF ? jx * qs : jx;
-  const R jyq = DEVF ? jy * qs : jy;
-  const R jx2 = jxq * jx, jy2 = jyq * jy, jz2 = (DEVF ? jz * qs : jz) * jz;
-  const R jj = (jx2 + jy2 + jz2);
-  const R e_eq = R(-11) * rho + R(19) * jj;
-  const R eps_eq = weps * rho + wepsj * jj;
-  const R pxx3_eq = R(2) * jx2 - (jy2 + jz2);
-  const R pww_eq = jy2 - jz2;
-  R dm[19];
-  dm[1] = s1 * (e - e_eq);
-  dm[2] = s2 * (eps - eps_eq);
-  dm[4] = s4 * (qx + R(2.) / R(3.) * jx);
-  dm[6] = s4 * (qy + R(2.) / R(3.) * jy);
-  dm[8] = s4 * (qz + R(2.) / R(3.) * jz);
-  dm[9] = s9 * (pxx3 - pxx3_eq);
-  dm[10] = s10 * (pixx3 - wxx * pxx3_eq);
-  dm[11] = s9 * (pww - pww_eq);
-  dm[12] = s10 * (piww - wxx * pww_eq);
-  dm[13] = s13 * (pxy - jxq * jy);
-  dm[14] = s13 * (pyz - jyq * jz);
-  dm[15] = s13 * (pxz - jxq * jz);
-  dm[16] = s16 * m[16];
-  dm[17] = s16 * m[17];
-  dm[18] = s16 * m[18];
-  // back-transform of the changes: rest direction, then opposite pairs
+  const V s9 = L::splat(T(p.inv_tau)), s13 = s9;
+  const V s1 = L::splat(T(p.mrt[0])), s2 = L::splat(T(p.mrt[1])), s4 = L::splat(T(p.mrt[2]));
+  const V s10 = L::splat(T(p.mrt[3])), s16 = L::splat(T(p.mrt[4]));
+  const V weps = L::splat(T(p.mrt[5])), wepsj = L::splat(T(p.mrt[6])), mwxx = L::splat(-T(p.mrt[7]));
+  // DEVF: a product of two scaled momenta carries one scale too many
+  const V qs = L::splat(DEVF ? T(p.inv_scale) : T(1));
+  const V jxq = DEVF ? L::mul(jx, qs) : jx;
+  const V jyq = DEVF ? L::mul(jy, qs) : jy;
+  const V jzq = DEVF ? L::mul(jz, qs) : jz;
+  const V jx2 = L::mul(jxq, jx), jy2 = L::mul(jyq, jy), jz2 = L::mul(jzq, jz);
+  const V jj = L::add(L::add(jx2, jy2), jz2);
+  const V e_eq = L::fma(L::splat(T(19)), jj, L::mul(L::splat(T(-11)), rho));
+  const V eps_eq = L::fma(wepsj, jj, L::mul(weps, rho));
+  const V pxx3_eq = L::sub(L::add(jx2, jx2), L::add(jy2, jz2));
+  const V pww_eq = L::sub(jy2, jz2);
+  const V two3 = L::splat(T(2) / T(3));
+  V dm[19];
+  dm[1] = L::mul(s1, L::sub(e, e_eq));
+  dm[2] = L::mul(s2, L::sub(eps, eps_eq));
+  dm[4] = L::mul(s4, L::fma(two3, jx, qx));
+  dm[6] = L::mul(s4, L::fma(two3, jy, qy));
+  dm[8] = L::mul(s4, L::fma(two3, jz, qz));
+  dm[9] = L::mul(s9, L::sub(pxx3, pxx3_eq));
+  dm[10] = L::mul(s10, L::fma(mwxx, pxx3_eq, pixx3));
+  dm[11] = L::mul(s9, L::sub(pww, pww_eq));
+  dm[12] = L::mul(s10, L::fma(mwxx, pww_eq, piww));
+  dm[13] = L::mul(s13, L::sub(pxy, L::mul(jxq, jy)));
+  dm[14] = L::mul(s13, L::sub(pyz, L::mul(jyq, jz)));
+  dm[15] = L::mul(s13, L::sub(pxz, L::mul(jxq, jz)));
+  dm[16] = L::mul(s16, m[16]);
+  dm[17] = L::mul(s16, m[17]);
+  dm[18] = L::mul(s16, m[18]);
+  // back-transform of the changes: rest direction, then opposite pairs; + 3 rho w_i e_i.F with
+  // the full density (3 w_i e_i.F from the plan)
   auto part = [&]<int I, bool WANT_EVEN>() {
-    R acc = R(0);
+    V acc{};
     bool first = true;
     Unroll<0, 19>::run([&]<int K>() {
       constexpr int num = MrtTables::BN[I][K];
       if constexpr (num != 0 && !mrt_conserved(K) && mrt_even(K) == WANT_EVEN) {
-        constexpr R coef = R(num) / R(mrt_den<I>(K));
-        acc = first ? coef * dm[K] : fmar(coef, dm[K], acc);
+        constexpr T coef = T(num) / T(mrt_den<I>(K));
+        acc = first ? L::mul(L::splat(coef), dm[K]) : L::fma(L::splat(coef), dm[K], acc);
         first = false;
       }
     });
     return acc;
   };
-  const bool force = p.has_force != 0;
-  const R Fx = R(p.F[0]), Fy = R(p.F[1]), Fz = R(p.F[2]);
-  const R frho = R(3.) * (DEVF ? R(p.scale) * (R(p.rho0) + rho * qs) : rho);
-  v[0] = v[0] - part.template operator()<0, true>();
+  v[0] = L::sub(v[0], part.template operator()<0, true>());
   Unroll<1, 10>::run([&]<int P>() {
     constexpr int A = 2 * P - 1, B = 2 * P;
-    const R E = part.template operator()<A, true>();
-    const R O = part.template operator()<A, false>();
-    v[A] = v[A] - (E + O);
-    v[B] = v[B] - (E - O);
-    if (force) {
-      v[A] = fmar(frho * weight<R, A>(), edot<A, R>(Fx, Fy, Fz), v[A]);
-      v[B] = fmar(frho * weight<R, B>(), edot<B, R>(Fx, Fy, Fz), v[B]);
-    }
+    const V E = part.template operator()<A, true>();
+    const V O = part.template operator()<A, false>();
+    v[A] = L::sub(v[A], L::add(E, O));
+    v[B] = L::sub(v[B], L::sub(E, O));
   });
+  if (p.has_force != 0) {  // + 3 rho w_i e_i.F with the full density (3 w_i e_i.F from the plan)
+    const V fr = DEVF ? L::mul(L::splat(T(p.scale)), L::fma(rho, qs, L::splat(T(p.rho0)))) : rho;
+    Unroll<1, Q>::run([&]<int I>() {
+      const T fw = sizeof(T) == 8 ? T(p.fw3[I]) : T(p.ffw3[I]);
+      v[I] = L::fma(L::splat(fw), fr, v[I]);
+    });
+  }
 }
 
 // ------------------------------------------------------------------ Zou/He planes
@@ -786,63 +850,95 @@ __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, 
 }
 
 // ------------------------------------------------------------------ one node of the step
-// COLL: 0 BGK, 1 MRT, 2 chosen at run time by p.collision (mixed batches, read-out modes).
-template <typename R, bool STRICT, int COLL>
-__device__ __forceinline__ void collide(R (&v)[Q], const StepPlan& p) {
-  if (COLL == 0 || (COLL == 2 && p.collision == 0))
-    bgk<R, STRICT>(v, p);
-  else if constexpr (STRICT)
-    mrt<R, true>(v, p);
-  else
-    mrt_fast<R, false>(v, p);
-}
-
-// BGK on scaled deviations v_i = scale * (f_i - w_i rho0) (w_i rho0 is the BGK storage reference):
-// rho = rho0 + sum v / scale, u = (sum e v) / (scale rho), and per direction
-// v_i <- (1 - 1/tau) v_i + (1/tau) w_i (sum v + scale rho P_i), P_i = e.u (3 + 4.5 e.u) - 1.5 u^2.
-// Every sum runs over small numbers, so FP32 keeps the deviations' own precision and its rounding
-// does not accumulate into the mass the way a sum of full populations does.
-template <typename R>
-__device__ __forceinline__ void bgk_dev(R (&v)[Q], const StepPlan& p) {
-  R drs = v[0];
-#pragma unroll
-  for (int i = 1; i < Q; i++) drs = drs + v[i];
-  const R jx = ((((((((v[1] - v[2]) + v[7]) - v[8]) + v[9]) - v[10]) + v[11]) - v[12]) + v[13]) - v[14];
-  const R jy = ((((((((v[3] - v[4]) + v[7]) - v[8]) - v[9]) + v[10]) + v[15]) - v[16]) + v[17]) - v[18];
-  const R jz = ((((((((v[5] - v[6]) + v[11]) - v[12]) - v[13]) + v[14]) + v[15]) - v[16]) - v[17]) + v[18];
-  // every product that meets an addition is an explicit fmaf or a __fmul_rn, which the compiler
-  // never contracts: the kernels that inline this code round identically
-  const R rho = fmaf(drs, R(p.inv_scale), R(p.rho0));
-  const R srho = R(p.scale) * rho;
-  const R cu = R(1) / srho;
-  const R ux = __fmul_rn(jx, cu), uy = __fmul_rn(jy, cu), uz = __fmul_rn(jz, cu);
-  const R c15 = R(1.5) * fmaf(ux, ux, fmaf(uy, uy, __fmul_rn(uz, uz)));
-  const R om = R(p.inv_tau), om1 = R(1) - om;
-  // feq_i / w_i = drs + srho P_i = base + eu (s3 + s45 eu)
-  const R base = fmaf(-srho, c15, drs);
-  const R s3 = R(3.) * srho, s45 = R(4.5) * srho;
-  const R omw[3] = {om * weight<R, 0>(), om * weight<R, 1>(), om * weight<R, 7>()};
-  Unroll<0, Q>::run([&]<int I>() {
-    constexpr int wc = I == 0 ? 0 : (I < 7 ? 1 : 2);
-    R g = base;
-    if constexpr (I != 0) {
-      const R eu = edot<I, R>(ux, uy, uz);
-      g = fmaf(eu, fmaf(eu, s45, s3), base);
-    }
-    v[I] = fmaf(omw[wc], g, __fmul_rn(om1, v[I]));
+// BGK of every tier except FP64, over one node or a node pair.
+// DEVF (16-bit storage): v holds scaled deviations v_i = scale * (f_i - w_i rho0) (w_i rho0 is the
+// BGK storage reference): rho = rho0 + sum v / scale, u = (sum e v) / (scale rho), and per
+// direction v_i <- (1 - 1/tau) v_i + (1/tau) w_i (sum v + scale rho P_i),
+// P_i = e.u (3 + 4.5 e.u) - 1.5 u^2.  Every sum runs over small numbers, so FP32 keeps the
+// deviations' own precision and its rounding does not accumulate into the mass the way a sum of
+// full populations does.
+// !DEVF (FP32 storage): v holds full populations; the same update with sum v = rho, scale = 1
+// and rho0 = 0 is f_i <- (1 - 1/tau) f_i + (1/tau) feq_i, u = j / rho where rho > 1e-14
+// (macro_variables.hpp:56-69), else u = j.
+// feq_i / w_i - (sum v) = srho P_i is folded to two FMAs per direction: with eu = e_I.u for the
+// odd direction I, g_I = base + eu (s3 + s45 eu) and g_{I+1} = base + eu (s45 eu - s3).
+// The sums run over the opposite pairs: sum = v_0 + sum_p S_p and j_ax = sum_p e_{2p-1}[ax] D_p
+// in increasing p (the first term is p = ax + 1: directions 1, 3, 5, component +1).
+template <typename V, bool DEVF>
+__device__ __forceinline__ void bgk_v(V (&v)[Q], const StepPlan& p) {
+  using L = Lanes<V>;
+  using T = typename L::S;
+  V sum = v[0], jx, jy, jz;
+  Unroll<1, 10>::run([&]<int P>() {
+    constexpr int I = 2 * P - 1;
+    const V a = v[I], b = v[I + 1];
+    const V d = L::sub(a, b);
+    sum = L::add(sum, L::add(a, b));
+    auto acc = [&]<int C, int FIRST>(V& j) {
+      if constexpr (P == FIRST) j = d;
+      else if constexpr (C > 0) j = L::add(j, d);
+      else if constexpr (C < 0) j = L::sub(j, d);
+    };
+    acc.template operator()<D3Q19::ex[I], 1>(jx);
+    acc.template operator()<D3Q19::ey[I], 2>(jy);
+    acc.template operator()<D3Q19::ez[I], 3>(jz);
   });
-  if (p.has_force != 0) {
-    const R Fx = __fmul_rn(s3, R(p.F[0])), Fy = __fmul_rn(s3, R(p.F[1])), Fz = __fmul_rn(s3, R(p.F[2]));
-    Unroll<1, Q>::run([&]<int I>() { v[I] = fmaf(weight<R, I>(), edot<I, R>(Fx, Fy, Fz), v[I]); });
+  V srho, cu;
+  if constexpr (DEVF) {
+    const V rho = L::fma(sum, L::splat(T(p.inv_scale)), L::splat(T(p.rho0)));
+    srho = L::mul(L::splat(T(p.scale)), rho);
+    cu = L::rcp(srho);
+  } else {
+    srho = sum;
+    V r = L::rcp(sum);
+    Unroll<0, L::N>::run([&]<int K>() {  // macro_variables: no division at vanishing density
+      if (!(L::lane(sum, K) > T(1.0e-14))) r = L::select(1 << K, L::splat(T(1)), r);
+    });
+    cu = r;
   }
+  const V ux = L::mul(jx, cu), uy = L::mul(jy, cu), uz = L::mul(jz, cu);
+  const V c15 = L::mul(L::splat(T(1.5)), L::fma(ux, ux, L::fma(uy, uy, L::mul(uz, uz))));
+  const T om = T(p.inv_tau);
+  const V om1 = L::splat(T(1) - om);
+  const V base = L::fma(L::mul(L::splat(T(-1)), srho), c15, sum);
+  const V s3 = L::mul(L::splat(T(3.)), srho), ms3 = L::mul(L::splat(T(-3.)), srho);
+  const V s45 = L::mul(L::splat(T(4.5)), srho);
+  v[0] = L::fma(L::splat(om * weight<T, 0>()), base, L::mul(om1, v[0]));
+  Unroll<1, 10>::run([&]<int P>() {
+    constexpr int I = 2 * P - 1;
+    const V omw = L::splat(om * weight<T, I>());
+    const V eu = edot_odd<I, V>(ux, uy, uz);
+    const V gA = L::fma(eu, L::fma(eu, s45, s3), base);
+    const V gB = L::fma(eu, L::fma(eu, s45, ms3), base);
+    v[I] = L::fma(omw, gA, L::mul(om1, v[I]));
+    v[I + 1] = L::fma(omw, gB, L::mul(om1, v[I + 1]));
+  });
+  if (p.has_force != 0)  // + 3 rho w_i e_i.F (bgk.hpp:58), 3 w_i e_i.F from the plan
+    Unroll<1, Q>::run([&]<int I>() { v[I] = L::fma(L::splat(p.ffw3[I]), srho, v[I]); });
 }
 
-template <typename R, int COLL>
-__device__ __forceinline__ void collide_dev(R (&v)[Q], const StepPlan& p) {
-  if (COLL == 0 || (COLL == 2 && p.collision == 0))
-    bgk_dev<R>(v, p);
-  else
-    mrt_fast<R, true>(v, p);
+// The collision of a tier.  COLL: 0 BGK, 1 MRT, 2 chosen at run time
+// by p.collision (mixed batches, read-out modes).  FP64 keeps the reference's BGK structure
+// (strict: its operation order and divisions; otherwise FMA and reciprocal multiplies) and strict
+// FP64 the reference's MRT; the other tiers run bgk_v / mrt_fast, on one node (V = R) or a node
+// pair (V = float2).  DEV: the values are the scaled deviations of the 16-bit tiers.
+template <typename R, bool STRICT, int COLL, bool DEV, typename V>
+__device__ __forceinline__ void collide(V (&v)[Q], const StepPlan& p) {
+  const bool use_bgk = COLL == 0 || (COLL == 2 && p.collision == 0);
+  if constexpr (sizeof(R) == 8) {
+    static_assert(sizeof(V) == 8, "FP64 collides one node at a time");
+    if (use_bgk)
+      bgk<R, STRICT>(v, p);
+    else if constexpr (STRICT)
+      mrt<R, true>(v, p);
+    else
+      mrt_fast<V, false>(v, p);
+  } else {
+    if (use_bgk)
+      bgk_v<V, DEV>(v, p);
+    else
+      mrt_fast<V, DEV>(v, p);
+  }
 }
 
 // Whether node (x, y, z) lies on a face whose boundary operators can change it (p.face_mask).
@@ -876,20 +972,26 @@ __device__ __forceinline__ void node_update(R (&v)[Q], const S* __restrict__ fin
     for (int s = 0; s < p.nsets; s++) {  // start_iteration: set_distribution boxes
       const SetBox& b = p.sets[s];
       if (x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2])
-        Unroll<0, Q>::run([&]<int I>() {
-          if constexpr (DEV)
-            v[I] = (__fmul_rn(R(b.value), weight<R, I>()) - R(p.dref[I])) * R(p.scale);
-          else
-            v[I] = R(b.value) * weight<R, I>();
-        });
+        Unroll<0, Q>::run([&]<int I>() { v[I] = set_value<S, R, I>(b.value, p); });
     }
-    if (flag == FLAG_FLUID) {
-      if constexpr (DEV)
-        collide_dev<R, COLL>(v, p);
-      else
-        collide<R, STRICT, COLL>(v, p);
-    }
+    if (flag == FLAG_FLUID) collide<R, STRICT, COLL, DEV>(v, p);
   }
+}
+
+// node_update for two nodes a and b of a 4- or 2-byte tier, the two lanes of v: a first step
+// (MODE_PROLOGUE) or a fused step collides both lanes; a read-out (MODE_FINISH) leaves them.  The
+// pair kernels take lattices whose non-fluid nodes are walls under wall_bounce_back
+// (pair_kernels_apply): a wall node's populations are scratch that no fluid node reads, so it
+// collides with its partner and then stores the read-out value of a wall.  No boundary operators
+// (a face pass applies them) and no start_iteration boxes (plans with boxes run the one-node
+// kernel).  Each fluid lane gets exactly the arithmetic node_update gives its node.
+template <typename S, int MODE, int COLL>
+__device__ __forceinline__ void pair_update(float2 (&v)[Q], const StepPlan& p, int8_t fa, int8_t fb) {
+  constexpr bool DEV = is_16bit<S>();
+  if constexpr (MODE != MODE_FINISH) collide<float, false, COLL, DEV>(v, p);
+  const int wall = int(fa == FLAG_WALL) | int(fb == FLAG_WALL) << 1;
+  if (wall)
+    Unroll<0, Q>::run([&]<int I>() { v[I] = Lanes<float2>::select(wall, Lanes<float2>::splat(wall_value<S, I>(p)), v[I]); });
 }
 
 // The stored values the node (x, y, z) gathers (pull with periodic wrap and on-node bounce-back;
@@ -1031,17 +1133,16 @@ __global__ void __launch_bounds__(256, MINB) k_step_pairs(const S* __restrict__ 
   S ra[Q], rb[Q];
   node_gather<S, MODE, WALLS>(fin, flags, p, x, y, z, idx, ra);
   node_gather<S, MODE, WALLS>(fin, flags, p, xb, yb, z, idx + 1, rb);
-  R a[Q], b[Q];
-  Unroll<0, Q>::run([&]<int I>() {
-    a[I] = load_value<S, R, I>(ra[I], p);
-    b[I] = load_value<S, R, I>(rb[I], p);
-  });
-  node_update<S, R, STRICT, MODE, COLL>(a, fin, idx, x, y, z, fa, p, false, false);
-  node_update<S, R, STRICT, MODE, COLL>(b, fin, idx + 1, xb, yb, z, fb, p, false, false);
-  if (WALLS && fa == FLAG_WALL) Unroll<0, Q>::run([&]<int I>() { a[I] = -R(p.dref[I]) * R(p.scale); });
-  if (WALLS && fb == FLAG_WALL) Unroll<0, Q>::run([&]<int I>() { b[I] = -R(p.dref[I]) * R(p.scale); });
-  store_pair<S, R, MODE>(a, b, p, launch_seed<S>(p), idx,
-                         [&]<int I>(uint32_t w) { *reinterpret_cast<uint32_t*>(fout + I * p.stride + idx) = w; });
+  float2 v[Q];  // node a in .x, node b in .y
+  Unroll<0, Q>::run([&]<int I>() { v[I] = make_float2(load_value<S, R, I>(ra[I], p), load_value<S, R, I>(rb[I], p)); });
+  pair_update<S, MODE, COLL>(v, p, fa, fb);
+  const bool sr = MODE != MODE_FINISH && p.rounding;
+  uint32_t h = 0, h2 = 0;
+  if (sr) {
+    h = node_hash(idx, launch_seed<S>(p));
+    h2 = second_hash(h);
+  }
+  pack_pair<S>(v, sr, h, h2, [&]<int I>(uint32_t w) { *reinterpret_cast<uint32_t*>(fout + I * p.stride + idx) = w; });
 }
 
 // The face pass of the vectorised kernels: the nodes of the faces in `faces` (bit F = face F),

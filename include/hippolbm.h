@@ -196,9 +196,14 @@ int hlbm_put_flags(hlbm_ctx* ctx, const int8_t* in);
 int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
 /* Step kernel selection (no reference counterpart).  Variants 0..5: variant % 2 picks the kernel,
  * 0 = one node per thread (two per thread for the 16-bit tiers), 1 = vectorised (consecutive
- * x-nodes per thread in one vector per direction plane; used when nx splits into >= 32 vectors,
- * else the first kernel runs; with wall obstacles a fix-up pass re-steps the nodes next to walls); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256
- * threads per SM.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
+ * x-nodes per thread in one vector per direction plane -- 16 bytes at variant 1, 8 bytes at 3 and
+ * 5 for the FP32 and 16-bit tiers, 16 bytes always for FP64; used when nx splits into >= 32
+ * vectors, else the first kernel runs; with wall obstacles a fix-up pass re-steps the nodes next
+ * to walls); variant / 2 = 0, 1, 2 targets at least 1, 2 or 3 blocks of 256 threads per SM.
+ * The FP32 and 16-bit tiers update node pairs in packed FP32 where a plan has no body force, no
+ * start_iteration boxes and no wall nodes outside wall_bounce_back; other plans run one node per
+ * thread.  A context starts at its tier's default (hlbm_autotune's pick on 512^3 Couette: FP64 4,
+ * FP32 1, FP16 / BF16 5 with BGK and 3 with MRT) until hlbm_tune or hlbm_autotune chooses.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
  * into shared-memory stages (256 or 512 threads per CTA; needs nx * bytes per population to be a
  * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
  * variant on this lattice (from the current populations into the idle buffer, so the state does

@@ -529,13 +529,17 @@ static void mrt_cell(double* f, int64_t nc, int64_t idx, double tau, const doubl
   const double weps = r[5], wepsj = r[6], wxx = r[7];
   double fl[Q], m[19];
   for (int i = 0; i < Q; i++) fl[i] = f[i * nc + idx];
+  /* both loops are unrolled whole, so the table entries are constants: zero terms vanish and
+   * num / den folds to the same double the division gives at run time */
+#pragma GCC unroll 19
   for (int k = 0; k < 19; k++) {
     double acc = 0.0;
     int first = 1;
+#pragma GCC unroll 19
     for (int i = 0; i < Q; i++) {
-      int c = MROW[k][i];
+      const int c = MROW[k][i];
       if (c == 0) continue;
-      double term = (c == 1) ? fl[i] : (c == -1 ? -fl[i] : (double)c * fl[i]);
+      const double term = (c == 1) ? fl[i] : (c == -1 ? -fl[i] : (double)c * fl[i]);
       acc = first ? term : acc + term;
       first = 0;
     }
@@ -576,14 +580,16 @@ static void mrt_cell(double* f, int64_t nc, int64_t idx, double tau, const doubl
   mo[17] = my - s16 * my;
   mo[18] = mz - s16 * mz;
   /* back-transform, mrt.hpp:129-173 */
+#pragma GCC unroll 19
   for (int i = 0; i < Q; i++) {
     double acc = 0.0;
     int first = 1;
+#pragma GCC unroll 19
     for (int k = 0; k < 19; k++) {
       const frac c = BACK[i][k];
       if (c.num == 0) continue;
-      double coef = (double)(c.num < 0 ? -c.num : c.num) / (double)c.den;
-      double term = coef * mo[k];
+      const double coef = (double)(c.num < 0 ? -c.num : c.num) / (double)c.den;
+      const double term = coef * mo[k];
       if (first) {
         acc = c.num < 0 ? -term : term;
         first = 0;
