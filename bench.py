@@ -67,7 +67,8 @@ def parse_args():
     ap.add_argument("--autotune", action="store_true", help="time every variant on the lattice and keep the fastest")
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="16-bit storage rounding")
-    ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve"])
+    ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve", "parity"])
+    ap.add_argument("--parity-steps", type=int, default=500, help="parity workload: time steps")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="precision workload: linear scale of the 1024x256x256 channel (steps scale alike)")
     ap.add_argument("--tiers", default="f64,f32,f16,f16:nearest,bf16",
@@ -472,6 +473,48 @@ def run_serve(a):
     return 0
 
 
+def run_parity(a):
+    """The Couette workload (--n, --collision, --tau) on the CPU oracle and on the GPU in strict FP64
+    and FP64: strict FP64 must equal the oracle in every population, FP64 stay within 1e-12 of it
+    relative to each population.  The oracle is the C restatement of the reference (bit-exact
+    against the reference functors on every golden case), OpenMP over all host threads."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from hippolbm_b200 import deck
+    from hippolbm_b200.lattice import Lattice
+
+    case = deck.couette_case(a.n, tau=a.tau, u_wall=0.05, steps=a.parity_steps, collision=a.collision)
+    t0 = time.perf_counter()
+    ref = oracle.OracleLattice(case, "port").initialize().step(a.parity_steps)
+    t_oracle = time.perf_counter() - t0
+    f_ref = ref.real(ref.f())
+    out = {}
+    for precision in ("f64_strict", "f64"):
+        with Lattice.from_case(case, precision) as lat:
+            lat.step(a.parity_steps)
+            f = lat.populations()
+        mismatches, worst = 0, 0.0
+        for i in range(19):
+            a_i, b_i = f[i], f_ref[i]
+            mismatches += int(np.count_nonzero(a_i != b_i))
+            worst = max(worst, float((np.abs(a_i - b_i) / np.abs(b_i)).max()))
+        out[precision] = {"populations_differing": mismatches, "max_rel_diff": worst}
+        del f
+    ref.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", "0")) or (os.cpu_count() or 1)
+    line = {"workload": "parity", "metric": "max relative population difference (FP64 vs oracle)",
+            "value": out["f64"]["max_rel_diff"], "unit": "1", "higher_is_better": False, "n_gpus": 1,
+            "steps": a.parity_steps, "data": "synthetic",
+            "config": {"workload": workload_name(a), "nodes": [a.n] * 3, "collision": a.collision, "tau": a.tau},
+            "tolerance": 1e-12, "pass": out["f64_strict"]["populations_differing"] == 0
+            and out["f64"]["max_rel_diff"] <= 1e-12,
+            "by_precision": out, "oracle": {"kind": "port", "cores": cores, "seconds": round(t_oracle, 1)}}
+    print(json.dumps(line), flush=True)
+    return 0 if line["pass"] else 1
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -482,6 +525,8 @@ def main():
         return run_batch(a)
     if a.workload == "serve":
         return run_serve(a)
+    if a.workload == "parity":
+        return run_parity(a)
     return run_ours(a)
 
 

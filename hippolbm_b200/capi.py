@@ -69,6 +69,7 @@ SIGNATURES = {
     "hlbm_tune": (C.c_int, [_vp, C.c_int32]),
     "hlbm_autotune": (C.c_int, [_vp, C.c_int32, _i3, _d3]),
     "hlbm_stream": (_vp, [_vp]),
+    "hlbm_set_wait_limit": (C.c_int, [_vp, C.c_int64]),
     "hlbm_batch_create": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(_vp)]),
     "hlbm_batch_add": (C.c_int, [_vp, _vp]),
     "hlbm_batch_remove": (C.c_int, [_vp, _vp]),

@@ -126,6 +126,7 @@ struct hlbm_ctx {
   int8_t* nearwall = nullptr;  // per node: some pull comes from a wall node (k_near_wall)
   bool maybe_walls = false;     // the flags may hold wall nodes (an obstacle was rasterised or put)
   bool variant_tuned = false;   // hlbm_tune / hlbm_autotune chose the variant (else the tier default)
+  long long wait_limit = TMA_WAIT_LIMIT;  // polls before a wait of the pipelined kernel gives up
   double* partials = nullptr;
   double* stats_dev = nullptr;
   double* plane_tmp = nullptr;
@@ -404,6 +405,7 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   t.stages = t.ctas_per_sm == 2 ? c->tma_stages2 : c->tma_stages;
   t.parity = (fin == c->f[0]) ? 0 : 1;
   t.err = c->err_dev;
+  t.wait_limit = c->wait_limit;
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
   t.seed = p.seed;
   c->launches++;
@@ -1170,6 +1172,12 @@ int hlbm_info(hlbm_ctx* c, int64_t info[8]) {
   info[5] = c->launches;
   info[6] = int64_t(elem_size(c->precision));
   info[7] = c->device;
+  return HLBM_OK;
+}
+
+int hlbm_set_wait_limit(hlbm_ctx* c, int64_t polls) {
+  if (!c || polls < 0) return fail(HLBM_EINVAL, "hlbm_set_wait_limit: polls must be >= 0");
+  c->wait_limit = polls == 0 ? TMA_WAIT_LIMIT : polls;
   return HLBM_OK;
 }
 

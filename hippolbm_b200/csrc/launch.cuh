@@ -144,6 +144,7 @@ struct TmaArgs {
   int ctas_per_sm = 1;
   long long seed = -1;  // step number of a single-lattice launch; -1: the descriptors' counters
   int ndesc = 0;        // descriptors whose counters a batched launch advances
+  long long wait_limit = TMA_WAIT_LIMIT;  // polls before a pipeline wait gives up
 };
 
 template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
@@ -153,7 +154,7 @@ cudaError_t launch_tma_t(const TmaArgs& a, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   kern<<<a.grid, TMA_THREADS, smem, s>>>(a.desc, a.tiles, a.ntiles, a.tile_elems, a.parity, a.err, a.seed,
-                                                 a.ndesc);
+                                                 a.ndesc, a.wait_limit);
   return cudaGetLastError();
 }
 

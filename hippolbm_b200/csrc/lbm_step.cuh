@@ -554,11 +554,10 @@ __device__ __forceinline__ void pack_pair(const float2 (&v)[Q], bool sr, uint32_
 // first pair with a non-zero coefficient in moment row K (0: the rest direction).
 template <int K>
 constexpr int mrt_first_term() {
-  constexpr bool EV = mrt_even(K);
-  if (EV && MrtTables::M[K][0] != 0) return 0;
-  for (int P = 1; P < 10; P++)
-    if (MrtTables::M[K][2 * P - 1] != 0) return P;
-  return 10;
+  int first = 10;
+  for (int P = 9; P >= 1; P--)
+    if (MrtTables::M[K][2 * P - 1] != 0) first = P;
+  return (mrt_even(K) && MrtTables::M[K][0] != 0) ? 0 : first;
 }
 
 // The MRT collision of every tier except strict FP64, in about half the reference's operations.
@@ -994,17 +993,28 @@ __device__ __forceinline__ void pair_update(float2 (&v)[Q], const StepPlan& p, i
     Unroll<0, Q>::run([&]<int I>() { v[I] = Lanes<float2>::select(wall, Lanes<float2>::splat(wall_value<S, I>(p)), v[I]); });
 }
 
+template <typename S, bool WALLS>
+__device__ __forceinline__ void node_pull(const S* __restrict__ fin, const int8_t* __restrict__ flags,
+                                          const StepPlan& p, int x, int y, int z, int64_t idx, S (&raw)[Q]);
+
 // The stored values the node (x, y, z) gathers (pull with periodic wrap and on-node bounce-back;
 // in the prologue its own values), every load issued before any is used.  A bounced value (the
 // node's own opp(I) slot) decodes like a pulled one because the storage reference is symmetric.
 template <typename S, int MODE, bool WALLS>
 __device__ __forceinline__ void node_gather(const S* __restrict__ fin, const int8_t* __restrict__ flags,
                                             const StepPlan& p, int x, int y, int z, int64_t idx, S (&raw)[Q]) {
-  if (MODE == MODE_PROLOGUE) {
+  if constexpr (MODE == MODE_PROLOGUE) {
     Unroll<0, Q>::run([&]<int I>() { raw[I] = ld_stream(fin + I * p.stride + idx); });
-    return;
+  } else {
+    node_pull<S, WALLS>(fin, flags, p, x, y, z, idx, raw);
   }
-  // source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others flag "outside"
+}
+
+// node_gather's pull: source coordinates x - e for e in {+1, 0, -1}; periodic axes wrap, others
+// flag "outside" (on-node bounce-back), as do wall sources where wall_bounce_back is active.
+template <typename S, bool WALLS>
+__device__ __forceinline__ void node_pull(const S* __restrict__ fin, const int8_t* __restrict__ flags,
+                                          const StepPlan& p, int x, int y, int z, int64_t idx, S (&raw)[Q]) {
   int sx[3], sy[3], sz[3];
   bool ox[3], oy[3], oz[3];
 #pragma unroll

@@ -14,8 +14,9 @@
 // global memory with coalesced stores.
 //
 // Copies are plain (non-multicast) bulk loads of this GPU's own memory.  Every mbarrier wait is
-// bounded: on timeout the CTA records an error code in *err, waits (bounded) for the copies it
-// has in flight, and returns.
+// bounded: a work wait gives up after `wait_limit` polls (about a second by default), records an
+// error code in *err, and its warp returns; the producer then waits (bounded by the default
+// limit) for the copies it has in flight before the CTA exits.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -79,10 +80,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
                : "memory");
 }
 
-// polls the phase with the given parity; false if it did not complete within the limit
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// polls the phase with the given parity; false if it did not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit = TMA_WAIT_LIMIT) {
   const unsigned a = smem_addr(bar);
-  for (long long it = 0; it < TMA_WAIT_LIMIT; it++) {
+  for (long long it = 0; it < limit; it++) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -163,7 +164,7 @@ __device__ __forceinline__ void issue_direction(const LatticeDesc& L, const Step
 template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
 __global__ void __launch_bounds__(TMA_THREADS, MINB)
     k_step_tma(LatticeDesc* __restrict__ lats, const Tile* __restrict__ tiles, int ntiles, int tile_elems,
-               int parity, int* __restrict__ err, long long seed, int ndesc) {
+               int parity, int* __restrict__ err, long long seed, int ndesc, long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
   uint64_t* empty = full + STAGES;
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
     int k = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
       const int s = k % STAGES;
-      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1)) {  // consumers released s
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, wait_limit)) {  // consumers released s
         if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
         break;
       }
@@ -196,7 +197,8 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
       __syncwarp();
       if (lane < Q) issue_direction<S>(L, p, parity, tl, stages + s * stage_elems, tile_elems, &full[s], lane);
     }
-    // every copy issued must land before the CTA exits (bounded wait)
+    // every copy issued must land before the CTA exits (bounded by the full limit, whatever the
+    // work waits' limit: the copies of a stage land within microseconds)
     const int issued = k;
     for (int kk = issued - STAGES < 0 ? 0 : issued - STAGES; kk < issued; kk++)
       mbar_wait(&full[kk % STAGES], (kk / STAGES) & 1);
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(TMA_THREADS, MINB)
       asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory");
       plan_of = tl.x;
     }
-    if (!mbar_wait(&full[s], (k / STAGES) & 1)) {
+    if (!mbar_wait(&full[s], (k / STAGES) & 1, wait_limit)) {
       if (ctid == 0) atomicExch(err, TMA_ERR_TIMEOUT);
       return;
     }

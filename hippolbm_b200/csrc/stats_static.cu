@@ -11,10 +11,15 @@
 // The array is a file-scope __device__ object, so every GPU that loads this library holds it
 // (HLBM_STATIC_PARTIALS slots of 3 doubles, 384 KiB) until the process exits.  Host code
 // cannot use its name as a device address: the first call on each device, with that device
-// current, looks the address up with cudaGetSymbolAddress and caches it; make that first call
-// before any stream capture.  Each block writes its own slot before the second pass reads it,
-// so nothing needs clearing between calls, but every call shares the one array: calls that
-// overlap on the GPU (on different streams, say) race on it.
+// current, looks the address up with cudaGetSymbolAddress and caches it.  The address belongs
+// to the device's current CUDA context, so the cache also records that context's unique id and
+// looks the address up again when a call finds another context current (after a
+// cudaDeviceReset, or when a driver-API caller made its own context current).  Make the first
+// call on a device, and the first call after such a change, before any stream capture.  Each
+// block writes its own slot before the second pass reads it, so nothing needs clearing between
+// calls, but every call shares the one array: calls that overlap on the GPU (on different
+// streams, say) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,7 +40,33 @@ static __device__ __align__(256) double g_stats_partials[3 * kMaxPartials];
 
 constexpr int kMaxDevices = 64;
 double* g_partials_addr[kMaxDevices] = {nullptr};
+unsigned long long g_partials_ctx[kMaxDevices] = {0};  // unique id of the context the address is of
 std::mutex g_setup_mutex;
+
+// The unique id of the calling thread's current CUDA context (cuCtxGetId, reached through the
+// runtime's driver entry points so that the library needs no link against the driver library);
+// 0 when it cannot be read, in which case the cached address is kept.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* a = nullptr;
+    void* b = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, nullptr) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, nullptr) == cudaSuccess) {
+      get_current = reinterpret_cast<GetCurrent>(a);
+      get_id = reinterpret_cast<GetId>(b);
+    }
+    looked_up = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // Per-block sum of rho and extrema of |u| over one fixed range of kNodesPerBlock nodes (the
 // node ranges do not depend on the GPU, so the sum order is reproducible).  rho and u follow
@@ -141,16 +172,19 @@ extern "C" int hlbm_simulation_state_static(const double* f, int64_t stride, con
     return record_error(HLBM_ECUDA, "hlbm_simulation_state_static: no current CUDA device");
   double* partials = nullptr;
   {
-    // set-up, once per device, with that device current: the host-side name of the array is
-    // not a device address, so fetch the real one
+    // set-up, once per device (and again when another context is current on it), with that
+    // device current: the host-side name of the array is not a device address, so fetch the
+    // real one
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_partials_addr[dev] || (ctx != 0 && ctx != g_partials_ctx[dev])) {
       void* addr = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&addr, g_stats_partials);
       if (e != cudaSuccess)
         return record_error(HLBM_ECUDA, std::string("hlbm_simulation_state_static: cudaGetSymbolAddress: ") +
                                            cudaGetErrorString(e));
       g_partials_addr[dev] = static_cast<double*>(addr);
+      g_partials_ctx[dev] = current_context_id();  // the lookup makes the primary context current
     }
     partials = g_partials_addr[dev];
   }

@@ -214,6 +214,14 @@ int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
+/* Bound on each wait of the pipelined kernel (variants 6, 7) in polls of its shared-memory
+ * barrier; 0 restores the default of about a second.  No reference counterpart.  A wait that runs
+ * out records an error on the device and its CTA returns after its copies in flight have landed;
+ * the next call that reads the state (hlbm_get_populations, hlbm_simulation_state, ...) fails with
+ * HLBM_ECUDA and clears the record, and the context stays usable (put populations back and step
+ * on).  A small bound lets a test exercise that path, and a host that prefers to fail fast on a
+ * stalled GPU can shorten the default. */
+int hlbm_set_wait_limit(hlbm_ctx* ctx, int64_t polls);
 
 /* ---------------------------------------------------------------------------------------------
  * Batches (no reference counterpart).  A batch advances many independent lattices -- contexts
@@ -251,8 +259,10 @@ int hlbm_batch_destroy(hlbm_batch* b);
  * NULL; the call is asynchronous on it.  It allocates nothing: block partial sums go to a
  * static __device__ array of HLBM_STATIC_PARTIALS slots (384 KiB held by every GPU that
  * loads the library, until exit), so lattices above HLBM_STATIC_MAX_NODES nodes are rejected
- * with HLBM_EINVAL.  The first call on a device looks up the array's address (make it before
- * any stream capture).  All calls share the array: calls that overlap on the GPU race. */
+ * with HLBM_EINVAL.  The first call on a device looks up the array's address in the device's
+ * current context, and so does the first call after another context became current there (a
+ * cudaDeviceReset, or a driver-API caller's own context); make those calls before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
 #define HLBM_STATIC_PARTIALS 16384
 #define HLBM_STATIC_MAX_NODES (16384LL * HLBM_STATIC_PARTIALS)
 int hlbm_simulation_state_static(const double* f, int64_t stride, const int8_t* flags, const int32_t n[3],

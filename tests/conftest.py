@@ -29,6 +29,29 @@ def oracle_mod():
     return oracle
 
 
+def per_population_rel_err(f, f_ref, mask=None):
+    """max over populations of |f - f_ref| / |f_ref| (0 where both are 0), over the nodes of
+    `mask` (a boolean node array, or None for all).  Arrays are (19, nodes...); compared one
+    direction at a time so that lattices of billions of values need no full-size temporaries."""
+    import numpy as np
+
+    worst = 0.0
+    for i in range(f.shape[0]):
+        a = np.asarray(f[i], dtype=np.float64)
+        b = np.asarray(f_ref[i], dtype=np.float64)
+        if mask is not None:
+            a, b = a[mask], b[mask]
+        d = np.abs(a - b)
+        den = np.abs(b)
+        bad = (d > 0) & (den == 0)
+        if bad.any():
+            return float("inf")
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = np.where(den > 0, d / np.where(den > 0, den, 1.0), 0.0)
+        worst = max(worst, float(r.max()) if r.size else 0.0)
+    return worst
+
+
 def cuda_available() -> bool:
     try:
         import torch

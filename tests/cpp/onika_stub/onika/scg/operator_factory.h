@@ -1,0 +1,3 @@
+// see operator.h (test stand-in for Onika)
+#pragma once
+#include "operator.h"

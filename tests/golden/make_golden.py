@@ -11,7 +11,7 @@ Run in a container that has the reference tree (read-only) and oracle/_ref/libhl
   - the deck's check_macro_quantities pins.
 Small cases also store the real-box populations in golden_<name>.npz.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    HIPPOLBM_REFERENCE=<reference tree> python tests/golden/make_golden.py [--reference <reference tree>]
 """
 import argparse
 import glob
@@ -116,8 +116,11 @@ def run_reference(case):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("HIPPOLBM_REFERENCE"),
+                    help="the reference tree (default: $HIPPOLBM_REFERENCE)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set HIPPOLBM_REFERENCE to the reference tree")
     if not oracle.available("reference"):
         oracle.build("reference")
     cases = []

@@ -59,3 +59,22 @@ def test_reference_harness_agrees_when_available(oracle_mod):
     case = Case.from_dict(g["case"])
     lat = oracle_mod.OracleLattice(case, "reference").initialize().step(case.steps)
     assert sha(lat.real(lat.f()).copy()) == g["sha_f"]
+
+
+def test_port_equals_reference_functors_256(oracle_mod):
+    """The restatement against the reference's own functors on the 256^3 Couette lattice of the
+    large parity test (BGK and MRT, tau = 0.6, 5 steps): equal bit for bit at a size where
+    indices pass 2^24."""
+    from hippolbm_b200 import deck
+
+    if not oracle_mod.available("reference"):
+        pytest.skip("oracle/_ref (the reference functors) not built")
+    for collision in ("bgk", "mrt"):
+        case = deck.couette_case(256, tau=0.6, u_wall=0.05, steps=5, collision=collision)
+        a = oracle_mod.OracleLattice(case, "port").initialize().step(5)
+        b = oracle_mod.OracleLattice(case, "reference").initialize().step(5)
+        fa, fb = a.real(a.f()), b.real(b.f())
+        for i in range(19):
+            assert np.array_equal(fa[i], fb[i]), f"{collision}: direction {i} differs"
+        a.close()
+        b.close()
