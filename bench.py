@@ -18,10 +18,15 @@ launch per step for all of them, against the same lattices stepped one at a time
 path serving the same stream, one request at a time).
 
 The default arm prints one JSON line with the device-timed throughput (`value`), the end-to-end
-figure through the C-ABI with host buffers (`e2e`), the fused kernel's roofline against the
-measured HBM copy bandwidth, the CPU baseline (the reference's own functors, all host cores, a
-bounded sample), the SM clocks sampled during the timed region, and the number of kernel
-launches.  `--impl reference` times the reference functors alone (oracle/_ref) on the host.
+figure through the C-ABI with host buffers (`e2e`: populations in from pinned memory, the solve,
+rho and u of every node back out), the fused kernel's roofline against the measured HBM copy
+bandwidth, the CPU baseline (the reference's own functors, all host cores, the median of three
+segments on a 128^3 sample), the SM clocks sampled during the timed region, the number of kernel
+launches, and two summaries: `tiers` (the same 512^3 workload in FP64 MRT, FP32 and FP16 / BF16
+storage, BGK and MRT: ms per step, MLUPS, fraction of the copy bandwidth, kernel) and `serve` (16
+requests at 100 req/s served by continuous batching in FP16 against the plain FP64 path one at a
+time: p50 / p99 time to solution, aggregate MLUPS).  `--impl reference` times the reference
+functors alone (oracle/_ref) on the host, on the same 512^3 workload.
 Multi-GPU (torchrun): independent replicas, one lattice per rank, throughput summed over ranks
 and timed as the max over ranks.
 """
@@ -84,6 +89,11 @@ def parse_args():
     ap.add_argument("--alone-steps", type=int, default=200,
                     help="batch workload: steps per lattice of the one-at-a-time comparison")
     ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per stream")
+    ap.add_argument("--no-tiers", action="store_true",
+                    help="default workload: skip the other storage tiers and collisions of the `tiers` object")
+    ap.add_argument("--no-serve", action="store_true", help="default workload: skip the `serve` summary")
+    ap.add_argument("--serve-requests", type=int, default=16, help="default workload: requests of the serve summary")
+    ap.add_argument("--serve-rate", type=float, default=100.0, help="default workload: arrival rate (req/s) of it")
     ap.add_argument("--rates", default="10,100,1000", help="serve workload: arrival rates (req/s)")
     return ap.parse_args()
 
@@ -195,45 +205,104 @@ def ncu_traffic_per_node(precision: str, collision: str, kernel: str):
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_reference_mlups(n: int, steps: int, warmup: int, collision: str, tau: float):
+def cpu_reference_mlups(n: int, steps, warmup: int, collision: str, tau: float, runs: int = 3):
     """The reference's own functors (oracle/_ref) on all host cores; falls back to the C
-    restatement (oracle/_build) when the harness library is absent."""
+    restatement (oracle/_build) when the harness library is absent.  After `warmup` steps, `runs`
+    timed segments of `steps` steps each (or of the step counts in the list `steps`); returns the
+    median segment's MLUPS with every segment's MLUPS, the kind, the thread count and the total
+    timed seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from hippolbm_b200 import deck
 
     kind = "reference" if oracle.available("reference") else "port"
-    case = deck.couette_case(n, tau=tau, u_wall=0.05, steps=steps, collision=collision)
+    counts = list(steps) if isinstance(steps, (list, tuple)) else [int(steps)] * runs
+    case = deck.couette_case(n, tau=tau, u_wall=0.05, steps=sum(counts), collision=collision)
     lat = oracle.OracleLattice(case, kind).initialize()
     lat.step(warmup)
-    t0 = time.perf_counter()
-    lat.step(steps)
-    dt = time.perf_counter() - t0
+    segs = []
+    for k in counts:
+        t0 = time.perf_counter()
+        lat.step(k)
+        segs.append(time.perf_counter() - t0)
     lat.close()
     cores = int(os.environ.get("OMP_NUM_THREADS", "0")) or (os.cpu_count() or 1)
-    return n ** 3 * steps / dt / 1e6, kind, cores, dt
+    mlups = [n ** 3 * k / dt / 1e6 for k, dt in zip(counts, segs)]
+    return statistics.median(mlups), mlups, kind, cores, sum(segs)
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(a):
+    """The reference's functors on the headline workload itself (512^3 by default): W warm-up
+    steps, then K steps timed as three segments; the median segment is the value."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    n = a.cpu_n
-    mlups, kind, cores, dt = cpu_reference_mlups(n, a.steps, a.warmup, a.collision, a.tau)
-    sample = (f"couette {n}^3 {a.collision} tau={a.tau} FP64 in the reference's ghosted layout, "
-              f"{a.steps} steps after {a.warmup} warm-up, OpenMP static over {cores} host threads")
+    n = a.n
+    segs = [a.steps // 3 + (1 if i < a.steps % 3 else 0) for i in range(3)]  # K steps in three segments
+    segs = [k for k in segs if k > 0]
+    mlups, runs, kind, cores, dt = cpu_reference_mlups(n, segs, a.warmup, a.collision, a.tau)
+    sample = (f"couette {n}^3 {a.collision} tau={a.tau} FP64 in the reference's ghosted layout: {a.warmup} "
+              f"warm-up steps, then {a.steps} steps timed as segments of {segs} steps, median segment; OpenMP "
+              f"static over {cores} host threads")
     line = {"metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": round(dt / a.steps * 1e3, 4), "higher_is_better": True,
+            "warmup": a.warmup, "ms_per_step": round(n ** 3 / (mlups * 1e6) * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": workload_name(a), "sample_nodes": [n, n, n], "collision": a.collision,
-                       "tau": a.tau},
+            "config": {"workload": workload_name(a), "nodes": [n, n, n], "collision": a.collision, "tau": a.tau,
+                       "segments_mlups": [round(v, 3) for v in runs]},
             "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------ tiers and serving summaries
+TIERS = [("f64", "mrt"), ("f32", "bgk"), ("f32", "mrt"), ("f16", "bgk"), ("f16", "mrt"), ("bf16", "bgk")]
+
+
+def measure_tier(a, precision: str, collision: str, local: int, peak: float) -> dict:
+    """The headline workload at another storage tier / collision: the tier's default kernel
+    variant, W warm-up steps, K steps timed by CUDA events on the lattice's stream."""
+    import torch
+
+    from hippolbm_b200 import deck
+    from hippolbm_b200.lattice import Lattice
+
+    case = deck.couette_case(a.n, tau=a.tau, u_wall=0.05, steps=500, collision=collision)
+    variant = DEFAULT_VARIANT[(precision, collision)]
+    with Lattice.from_case(case, precision, device=local) as lat:
+        lat.tune(variant)
+        stream = torch.cuda.ExternalStream(lat.stream_handle(), device=torch.device("cuda", local))
+        lat.step(a.warmup)
+        lat.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lat.step(a.steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        nodes = lat.ncell
+    alg = 38 * BYTES_PER_POP[precision] + 1
+    gbs = nodes * alg / (ms * 1e-3) / 1e9
+    return {"precision": precision, "collision": collision, "ms_per_step": round(ms, 4),
+            "mlups": round(nodes / (ms * 1e-3) / 1e6, 1), "algorithmic_gbs": round(gbs, 1),
+            "frac": round(gbs / peak, 4), "algorithmic_bytes_per_node": alg,
+            "kernel": f"hlbm::{step_kernel_name(variant)}", "variant": variant}
+
+
+def serve_summary(a) -> dict:
+    """Continuous batching of a Poisson request stream (FP16 storage, HBM admission budget 160 GB)
+    against the plain FP64 path serving the same stream one request at a time."""
+    from hippolbm_b200 import serve
+
+    fast = serve.serve_batched(serve.make_stream(a.serve_rate, a.serve_requests), "f16", hbm_budget=160e9, variant=10)
+    plain = serve.serve_plain(serve.make_stream(a.serve_rate, a.serve_requests), "f64")
+    keep = ("p50_s", "p99_s", "mean_s", "wall_s", "aggregate_mlups", "converged")
+    return {"rate_per_s": a.serve_rate, "requests": a.serve_requests, "edges": [24, 192], "budgets": [500, 20000],
+            "batched_f16": {k: fast[k] for k in keep}, "plain_f64": {k: plain[k] for k in keep},
+            "mlups_ratio": round(fast["aggregate_mlups"] / plain["aggregate_mlups"], 3)}
 
 
 # ------------------------------------------------------------------ our arm
@@ -283,24 +352,31 @@ def run_ours(a):
     lat.close()
     del lat
 
-    # end to end through the C-ABI with host buffers: H2D of the initial populations from
-    # pinned memory, one solve of e2e_steps time steps, D2H of simulation_state.
+    # end to end through the C-ABI with host buffers: one solve = H2D of the initial populations
+    # from pinned memory, e2e_steps time steps, and D2H of the result -- the macroscopic fields
+    # rho and u of every node (macro_variables) and simulation_state -- into pinned memory.
     e2e = None
     lat = Lattice.from_case(case, a.precision, device=local)
     lat.rounding(a.rounding)
     lat.tune(variant)
     init = torch.empty(19 * nodes, dtype=torch.float64, pin_memory=True)
+    rho_out = torch.empty(nodes, dtype=torch.float64, pin_memory=True)
+    u_out = torch.empty(3 * nodes, dtype=torch.float64, pin_memory=True)
     w = [1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12  # rest equilibrium, rho = 1
     iv = init.numpy().reshape(19, nodes)
     for i in range(19):
         iv[i] = w[i]
     stats = (C.c_double * 3)()
     L = lat.L
+    dp = C.POINTER(C.c_double)
 
     def solve():
-        L.hlbm_put_populations(lat.h, C.cast(init.data_ptr(), C.POINTER(C.c_double)))
-        L.hlbm_step(lat.h, a.e2e_steps)
-        L.hlbm_simulation_state(lat.h, stats)
+        rc = L.hlbm_put_populations(lat.h, C.cast(init.data_ptr(), dp))
+        rc = rc or L.hlbm_step(lat.h, a.e2e_steps)
+        rc = rc or L.hlbm_macro_variables(lat.h, C.cast(rho_out.data_ptr(), dp), C.cast(u_out.data_ptr(), dp))
+        rc = rc or L.hlbm_simulation_state(lat.h, stats)
+        if rc:
+            raise RuntimeError(L.hlbm_last_error().decode())
 
     solve()  # warm-up solve
     barrier(world, device)
@@ -310,11 +386,15 @@ def run_ours(a):
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     t_e2e = dist_max(t_e2e, world, device)
+    h2d = 19 * nodes * 8
+    d2h = 4 * nodes * 8 + 24
     e2e = {"value": round(world * nodes * a.e2e_steps / t_e2e / 1e6, 3), "unit": "MLUPS",
-           "h2d_bytes_per_step": int(19 * nodes * 8), "d2h_bytes_per_step": 24,
-           "step": f"one solve: put_populations (pinned host) + {a.e2e_steps} time steps + simulation_state"}
+           "h2d_bytes_per_step": int(h2d / a.e2e_steps), "d2h_bytes_per_step": int(d2h / a.e2e_steps),
+           "steps_per_solve": a.e2e_steps, "h2d_bytes_per_solve": h2d, "d2h_bytes_per_solve": d2h,
+           "step": f"one solve: put_populations (pinned host) + {a.e2e_steps} time steps + macro_variables "
+                   f"(rho, u to pinned host) + simulation_state"}
     lat.close()
-    del init
+    del init, rho_out, u_out
 
     out = None
     if rank == 0:
@@ -330,11 +410,19 @@ def run_ours(a):
                 "algorithmic_bytes_per_node": alg_bytes_per_node, "kernel": f"hlbm::{kname} (MODE_FUSED)"}
         cpu = None
         if not a.no_cpu_baseline and world == 1:
-            cpu_steps = 160  # about 10 s of host work on 16 cores
-            mlups_c, kind, cores, dt = cpu_reference_mlups(a.cpu_n, cpu_steps, 2, a.collision, a.tau)
+            cpu_steps = 50  # three segments: about 10 s of host work on 16 cores
+            mlups_c, runs_c, kind, cores, dt = cpu_reference_mlups(a.cpu_n, cpu_steps, 2, a.collision, a.tau)
             cpu = {"value": round(mlups_c, 3), "unit": "MLUPS", "cores": cores, "kind": kind,
-                   "sample": f"couette {a.cpu_n}^3 {a.collision} tau={a.tau} FP64, {cpu_steps} steps "
-                             f"({dt:.1f} s) through the reference functors, OpenMP over {cores} threads"}
+                   "sample": f"couette {a.cpu_n}^3 {a.collision} tau={a.tau} FP64 (a {a.cpu_n}^3 sample of the "
+                             f"{a.n}^3 workload): 3 segments of {cpu_steps} steps ({dt:.1f} s), median segment, "
+                             f"through the reference functors, OpenMP over {cores} threads",
+                   "segments_mlups": [round(v, 3) for v in runs_c]}
+        tiers = None
+        if not a.no_tiers and world == 1:
+            tiers = [measure_tier(a, prec, coll, local, peak) for prec, coll in TIERS]
+            for t in tiers:
+                t["vs_f64_bgk"] = round(t["mlups"] / (nodes / (ms_per_step * 1e-3) / 1e6), 3)
+        serving = None if (a.no_serve or world > 1) else serve_summary(a)
         out = {"metric": "MLUPS", "value": round(mlups_total, 3), "unit": "MLUPS", "n_gpus": world,
                "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_per_step, 5),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision],
@@ -346,7 +434,7 @@ def run_ours(a):
                           "kernel_variant": variant,
                           "autotune_ms": {str(k): round(v, 4) for k, v in variant_ms.items()}},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches) * world,
-               "clocks": clk}
+               "clocks": clk, "tiers": tiers, "serve": serving}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
