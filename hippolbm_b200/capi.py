@@ -22,6 +22,8 @@ _d3 = C.POINTER(C.c_double)
 _i3 = C.POINTER(C.c_int32)
 _vp = C.c_void_p
 # name -> (restype, argtypes); every symbol include/hippolbm.h declares
+NUM_VARIANTS = 10  # HLBM_NUM_VARIANTS of include/hippolbm.h
+
 SIGNATURES = {
     "hlbm_last_error": (C.c_char_p, []),
     "hlbm_version": (C.c_char_p, []),

@@ -408,12 +408,20 @@ cudaError_t launch_with_plan(hlbm_ctx* c, int mode, const void* fin, void* fout,
   t.wait_limit = c->wait_limit;
   t.grid = std::min(c->ntiles, c->sms * t.ctas_per_sm);
   t.seed = p.seed;
+  t.rows = true;
+  t.sms = c->sms;
+  const int bytes = int(elem_size(c->precision));
   c->launches++;
-  if (face_pass_runs(p, walls, variant, mode == MODE_PROLOGUE, int(elem_size(c->precision))))
-    c->launches++;  // the face pass after the step kernel
-  if (walls && mode != MODE_PROLOGUE && variant < 6 && variant % 2 == 1 &&
-      vec_eligible_bytes(p, walls, int(elem_size(c->precision)), variant))
-    c->launches++;  // the wall fix-up after the vectorised kernel
+  if (rows_runs(p, variant, mode, bytes)) {  // the row pipeline, then the face pass and the wall fix-up
+    if (p.face_mask != 0) c->launches++;
+    if (walls) c->launches++;
+  } else {
+    if (variant >= 8) variant = 5;  // what launch_step runs for variants 8 and 9 here
+    if (face_pass_runs(p, walls, variant, mode == MODE_PROLOGUE, bytes))
+      c->launches++;  // the face pass after the step kernel
+    if (walls && mode != MODE_PROLOGUE && variant < 6 && variant % 2 == 1 && vec_eligible_bytes(p, walls, bytes, variant))
+      c->launches++;  // the wall fix-up after the vectorised kernel
+  }
   switch (c->precision) {
     case HLBM_F64: return step_f64(mode, walls, fin, fout, c->flags, p, s, variant, t);
     case HLBM_F64_STRICT: return step_f64_strict(mode, walls, fin, fout, c->flags, p, s, variant, t);
@@ -1205,6 +1213,7 @@ int hlbm_autotune(hlbm_ctx* c, int32_t reps, int32_t* chosen, double* ms_per_var
   for (int v = 0; v < NUM_VARIANTS; v++) {
     if (ms_per_variant) ms_per_variant[v] = -1.0;
     if (v < 6 && (v % 2) == 1 && !vec_applies(c, v)) continue;
+    if (v >= 8 && !rows_runs(c->plan, v, MODE_FUSED, int(elem_size(c->precision)))) continue;
     if (v >= 6 && c->tma_stages < 2) continue;
     cudaError_t e = launch_step_variant(c, MODE_FUSED, fin, fout, v);  // warm-up
     if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
@@ -1286,7 +1295,7 @@ void batch_drop_graph(hlbm_batch* b) {
 // from one captured graph.  Graph-replayed launches of the 16-bit tiers read their step number
 // (the stochastic-rounding salt) from a per-member device counter pair, so every member rounds
 // exactly as it does stepped alone.
-int concurrent_variant(const hlbm_ctx* c) { return c->variant < 6 ? c->variant : 4; }
+int concurrent_variant(const hlbm_ctx* c) { return (c->variant < 6 || c->variant >= 8) ? c->variant : 4; }
 
 int64_t concurrent_state(const hlbm_ctx* c) { return (c->plan_version * 2 + c->cur) * 16 + concurrent_variant(c); }
 

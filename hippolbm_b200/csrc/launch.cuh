@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "lbm_step_rows.cuh"
 #include "lbm_step_tiles.cuh"
 #include "lbm_step_tma.cuh"
 #include "lbm_step_vec.cuh"
@@ -129,7 +130,9 @@ cudaError_t launch_vec(int walls, const void* fin, void* fout, const int8_t* fla
 // threads per SM (__launch_bounds__ minimum blocks, which caps registers at 255, 128 or 85 per
 // thread).  Variants 6 and 7: the bulk-copy pipelined persistent kernel (lbm_step_tma.cuh), with
 // tiles of about 512 (variant 6) or 1024 (variant 7) nodes; fused steps only, when eligible.
-constexpr int NUM_VARIANTS = 8;
+// Variants 8 and 9 (single lattices): the row pipeline of the 16-bit tiers (lbm_step_rows.cuh),
+// two or one CTA per SM; fused steps only, when eligible, else variant 5.
+constexpr int NUM_VARIANTS = 10;
 
 // what the pipelined kernel needs besides the plan
 struct TmaArgs {
@@ -145,6 +148,8 @@ struct TmaArgs {
   long long seed = -1;  // step number of a single-lattice launch; -1: the descriptors' counters
   int ndesc = 0;        // descriptors whose counters a batched launch advances
   long long wait_limit = TMA_WAIT_LIMIT;  // polls before a pipeline wait gives up
+  bool rows = false;  // single lattice: variants 8 and 9 are the row pipeline (batches: tile kernels)
+  int sms = 148;      // SMs of the device
 };
 
 template <typename S, typename R, bool STRICT, int STAGES, bool WALLS, int MINB>
@@ -221,9 +226,82 @@ cudaError_t launch_tiles(const TmaArgs& a, int walls, int variant, cudaStream_t 
   return cudaGetLastError();
 }
 
+// The row pipeline (lbm_step_rows.cuh) for one lattice: variant 8 = two CTAs per SM, variant 9 =
+// one CTA per SM with deeper staging; the face pass and (with wall obstacles) the wall fix-up
+// follow.  Returns cudaErrorNotSupported when the lattice or the mode cannot take it.
+inline int rows_stages(const RowsGeometry& g, int ctas_per_sm) {
+  const size_t budget = size_t(227 * 1024) / size_t(ctas_per_sm) - 1024;
+  const size_t fit = (budget - 128) / g.stage_bytes;
+  return fit >= 4 ? 4 : int(fit);
+}
+
+template <typename S, int COLL, int STAGES, int MINB>
+cudaError_t launch_rows_t(const Planes<S>& pl, const int8_t* flags, const StepPlan& p, const RowsGeometry& g,
+                          const TmaArgs& a, cudaStream_t s) {
+  auto kern = k_step_rows<S, COLL, STAGES, MINB>;
+  const size_t smem = rows_smem_bytes(STAGES, g);
+  if (cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) return e;
+  const int grid = g.ntiles < a.sms * MINB ? g.ntiles : a.sms * MINB;
+  kern<<<grid, ROWS_THREADS, smem, s>>>(pl, flags, p, g, a.err, a.wait_limit);
+  return cudaGetLastError();
+}
+
+template <typename S, int COLL, int MINB>
+cudaError_t launch_rows_stages(int stages, const Planes<S>& pl, const int8_t* flags, const StepPlan& p,
+                               const RowsGeometry& g, const TmaArgs& a, cudaStream_t s) {
+  if (stages >= 4) return launch_rows_t<S, COLL, 4, MINB>(pl, flags, p, g, a, s);
+  if (stages == 3) return launch_rows_t<S, COLL, 3, MINB>(pl, flags, p, g, a, s);
+  return launch_rows_t<S, COLL, 2, MINB>(pl, flags, p, g, a, s);
+}
+
+template <typename S, typename R, bool STRICT>
+cudaError_t launch_rows(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
+                        cudaStream_t s, int variant, const TmaArgs& a) {
+  if constexpr (!is_16bit<S>()) {
+    return cudaErrorNotSupported;
+  } else {
+    if (mode != MODE_FUSED || !rows_eligible(p, int(sizeof(S)))) return cudaErrorNotSupported;
+    const RowsGeometry g = rows_geometry(p, int(sizeof(S)));
+    const int ctas = variant == 8 ? 2 : 1;
+    const int stages = rows_stages(g, ctas);
+    if (stages < 2) return cudaErrorNotSupported;
+    const S* fi = static_cast<const S*>(fin);
+    S* fo = static_cast<S*>(fout);
+    const Planes<S> pl = make_planes(fi, fo, p.stride);
+    cudaError_t e;
+    if (ctas == 2)
+      e = p.collision == 0 ? launch_rows_stages<S, 0, 2>(stages, pl, flags, p, g, a, s)
+                           : launch_rows_stages<S, 1, 2>(stages, pl, flags, p, g, a, s);
+    else
+      e = p.collision == 0 ? launch_rows_stages<S, 0, 1>(stages, pl, flags, p, g, a, s)
+                           : launch_rows_stages<S, 1, 1>(stages, pl, flags, p, g, a, s);
+    if (e) return e;
+    if ((e = launch_faces<S, R, STRICT, MODE_FUSED, false>(fi, fo, flags, p, s))) return e;
+    if (!walls) return cudaSuccess;
+    const unsigned wgrid = unsigned((p.ncell + 255) / 256);
+    if (p.collision == 0)
+      k_wall_fixup<S, R, STRICT, MODE_FUSED, 0><<<wgrid, 256, 0, s>>>(fi, fo, flags, p);
+    else
+      k_wall_fixup<S, R, STRICT, MODE_FUSED, 1><<<wgrid, 256, 0, s>>>(fi, fo, flags, p);
+    return cudaGetLastError();
+  }
+}
+
+// Whether a single-lattice launch of `variant` in `mode` runs the row pipeline; otherwise variants 8
+// and 9 run variant 5.
+inline bool rows_runs(const StepPlan& p, int variant, int mode, int bytes) {
+  if (variant < 8 || mode != MODE_FUSED || !rows_eligible(p, bytes)) return false;
+  return rows_stages(rows_geometry(p, bytes), variant == 8 ? 2 : 1) >= 2;
+}
+
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_step(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
                         cudaStream_t s, int variant, const TmaArgs& tma) {
+  if (variant >= 8 && tma.rows) {
+    if (rows_runs(p, variant, mode, int(sizeof(S))))
+      return launch_rows<S, R, STRICT>(mode, walls, fin, fout, flags, p, s, variant, tma);
+    variant = 5;
+  }
   if (variant >= 8) return launch_tiles<S, R, STRICT>(tma, walls, variant, s);
   if (variant >= 6) {
     if (mode == MODE_FUSED && tma.stages >= 2) return launch_tma<S, R, STRICT>(tma, walls, tma.ctas_per_sm, s);

@@ -92,11 +92,7 @@ struct Codec<__half, float> {
   __device__ static __forceinline__ __half encd(float d, const StepPlan&) {
     return __float2half_rn(d);
   }
-  // stochastic rounding of one value (the low half of a pair) and of a pair (lo, hi)
-  template <int I>
-  __device__ static __forceinline__ __half encd_sr(float d, const StepPlan&, uint32_t r) {
-    return __ushort_as_half((unsigned short)(cvt_rs_f16x2(0.0f, d, r) & 0xffffu));
-  }
+  // stochastic rounding of a pair (lo, hi)
   template <int I>
   __device__ static __forceinline__ uint32_t encd_sr2(float lo, float hi, uint32_t r) {
     return cvt_rs_f16x2(hi, lo, r);
@@ -123,10 +119,6 @@ struct Codec<__nv_bfloat16, float> {
   template <int I>
   __device__ static __forceinline__ __nv_bfloat16 encd(float d, const StepPlan&) {
     return __float2bfloat16_rn(d);
-  }
-  template <int I>
-  __device__ static __forceinline__ __nv_bfloat16 encd_sr(float d, const StepPlan&, uint32_t r) {
-    return __ushort_as_bfloat16((unsigned short)(cvt_rs_bf16x2(0.0f, d, r) & 0xffffu));
   }
   template <int I>
   __device__ static __forceinline__ uint32_t encd_sr2(float lo, float hi, uint32_t r) {
@@ -167,15 +159,6 @@ __device__ __forceinline__ uint32_t node_hash(int64_t idx, uint32_t seed) {
   return h;
 }
 
-// bits for direction I: the node hash times a per-direction odd constant, whose well-mixed high
-// half is folded into the low half, so that both 16-bit halves are usable random bits
-template <int I>
-__device__ __forceinline__ uint32_t dir_bits(uint32_t h) {
-  constexpr uint32_t K = 0x9E3779B9u * (2u * I + 1u);
-  const uint32_t r = h * K;
-  return r ^ (r >> 16);
-}
-
 // Random bits for the pair conversion of direction I from two independent hash words: one IMAD.
 // The high half-word is the well-mixed top of h * K; the low half-word is a bijection of h's low
 // bits plus h2's, so it is uniform and, between two directions, the offset is independent of the
@@ -195,6 +178,22 @@ constexpr bool is_16bit() {
   return sizeof(S) == 2;
 }
 
+// One value of a node pair rounded as the pair conversion rounds it: the pair of node idx is
+// (idx & ~1, idx | 1), its random bits are pair_bits of the pair's first node, and the value takes
+// the half-word of those bits its lane takes (low for the even node, high for the odd one).  Every
+// kernel -- one node, two nodes or vectors per thread -- so rounds every value with the same
+// random bits, and the stochastically rounded state does not depend on the kernel that stepped it.
+template <typename S, int I>
+__device__ __forceinline__ S encd_sr_lane(float d, int64_t idx, uint32_t h, uint32_t h2) {
+  const uint32_t r = pair_bits<I>(h, h2);
+  const bool odd = (idx & 1) != 0;
+  const uint32_t w = Codec<S, float>::template encd_sr2<I>(odd ? 0.0f : d, odd ? d : 0.0f, r);
+  const unsigned short b = (unsigned short)(odd ? (w >> 16) : (w & 0xffffu));
+  S out;
+  memcpy(&out, &b, 2);
+  return out;
+}
+
 // ------------------------------------------------------------------ compile-time loops
 template <int I, int N>
 struct Unroll {
@@ -212,14 +211,16 @@ struct Unroll<N, N> {
 
 // Stores the node's Q values to dst(I).  FP64 / FP32 tiers carry full populations; the 16-bit
 // tiers carry deviations from the storage reference, rounded stochastically when the state is
-// carried (MODE_PROLOGUE / MODE_FUSED with p.rounding), else to nearest.  The branch is taken
-// once per node: selecting per value would make the compiler evaluate both conversions.
+// carried (MODE_PROLOGUE / MODE_FUSED with p.rounding; the bits of the node's pair,
+// encd_sr_lane), else to nearest.  The branch is taken once per node: selecting per value would
+// make the compiler evaluate both conversions.
 template <typename S, typename R, int MODE, class Dst>
 __device__ __forceinline__ void store_node(const R (&v)[Q], const StepPlan& p, uint32_t seed, int64_t idx, Dst&& dst) {
   if constexpr (is_16bit<S>()) {
     if (MODE != MODE_FINISH && p.rounding) {
-      const uint32_t h = node_hash(idx, seed);
-      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd_sr<I>(v[I], p, dir_bits<I>(h))); });
+      const uint32_t h = node_hash(idx & ~int64_t(1), seed);
+      const uint32_t h2 = second_hash(h);
+      Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(encd_sr_lane<S, I>(float(v[I]), idx, h, h2)); });
     } else {
       Unroll<0, Q>::run([&]<int I>() { dst.template operator()<I>(Codec<S, R>::template encd<I>(v[I], p)); });
     }

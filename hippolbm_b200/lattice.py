@@ -227,9 +227,9 @@ class Lattice:
         """Time every step-kernel variant on this lattice (state unchanged) and keep the fastest;
         returns (chosen variant, {variant: ms per step})."""
         chosen = C.c_int32(0)
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * capi.NUM_VARIANTS)()
         capi.check(self.L.hlbm_autotune(self.h, int(reps), C.byref(chosen), ms))
-        return chosen.value, {v: ms[v] for v in range(8) if ms[v] >= 0}
+        return chosen.value, {v: ms[v] for v in range(capi.NUM_VARIANTS) if ms[v] >= 0}
 
     def stream_handle(self) -> int:
         return self.L.hlbm_stream(self.h) or 0

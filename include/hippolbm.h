@@ -208,8 +208,12 @@ int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
  * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
  * variant on this lattice (from the current populations into the idle buffer, so the state does
  * not advance), keeps the fastest, and returns it in *chosen and the per-variant times (ms, -1 if
- * skipped) in ms_per_variant[HLBM_NUM_VARIANTS]. */
-#define HLBM_NUM_VARIANTS 8
+ * skipped) in ms_per_variant[HLBM_NUM_VARIANTS].  Variants 8, 9 (FP16 / BF16): the row pipeline --
+ * a producer warp bulk-copies each tile's source rows and flags into shared-memory stages, eight
+ * consumer warps update node pairs from there in packed FP32 -- with two (8) or one (9) CTA per
+ * SM; fused steps of lattices with nx % 16 == 0 and the pair kernels' plan conditions, else
+ * variant 5 runs. */
+#define HLBM_NUM_VARIANTS 10
 int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
