@@ -35,6 +35,14 @@ class Batch:
         capi.check(self.L.hlbm_batch_tune(self.h, int(variant)))
         return self
 
+    def autotune(self, reps: int = 3):
+        """Time one step of every batch variant on these members (no member's state advances) and
+        keep the fastest; returns (chosen variant, {variant: ms per step})."""
+        chosen = C.c_int32(0)
+        ms = (C.c_double * capi.BATCH_VARIANTS)()
+        capi.check(self.L.hlbm_batch_autotune(self.h, int(reps), C.byref(chosen), ms))
+        return chosen.value, {6 + k: ms[k] for k in range(capi.BATCH_VARIANTS) if ms[k] >= 0}
+
     def info(self) -> dict:
         out = (C.c_int64 * 6)()
         capi.check(self.L.hlbm_batch_info(self.h, out))

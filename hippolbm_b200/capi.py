@@ -23,6 +23,7 @@ _i3 = C.POINTER(C.c_int32)
 _vp = C.c_void_p
 # name -> (restype, argtypes); every symbol include/hippolbm.h declares
 NUM_VARIANTS = 10  # HLBM_NUM_VARIANTS of include/hippolbm.h
+BATCH_VARIANTS = 5  # HLBM_BATCH_VARIANTS: batch variants 6 .. 10
 
 SIGNATURES = {
     "hlbm_last_error": (C.c_char_p, []),
@@ -77,6 +78,7 @@ SIGNATURES = {
     "hlbm_batch_remove": (C.c_int, [_vp, _vp]),
     "hlbm_batch_step": (C.c_int, [_vp, C.c_int64]),
     "hlbm_batch_tune": (C.c_int, [_vp, C.c_int32]),
+    "hlbm_batch_autotune": (C.c_int, [_vp, C.c_int32, _i3, _d3]),
     "hlbm_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "hlbm_batch_stream": (_vp, [_vp]),
     "hlbm_batch_destroy": (C.c_int, [_vp]),

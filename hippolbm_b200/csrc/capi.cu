@@ -504,11 +504,12 @@ const char* hlbm_version(void) { return "hippolbm-b200 0.1.0 (sm_100a)"; }
 
 // Default step-kernel variant of a tier and collision: hlbm_autotune's pick on 512^3 Couette on a
 // B200.  FP64: one node per thread at >= 3 blocks/SM (4); FP32: 16-byte vectors at one block/SM
-// (1); FP16 / BF16: 8-byte vectors at >= 3 blocks/SM (5) for BGK, >= 2 blocks/SM (3) for MRT.
+// (1); FP16 / BF16: the row pipeline at two CTAs/SM (8) for BGK, one CTA/SM (9) for MRT (lattices
+// the row pipeline does not take run variant 5).
 static int default_variant(int precision, int collision) {
   if (precision == HLBM_F64 || precision == HLBM_F64_STRICT) return 4;
   if (precision == HLBM_F32) return 1;
-  return collision == 1 ? 3 : 5;
+  return collision == 1 ? 9 : 8;
 }
 
 int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],
@@ -1655,6 +1656,104 @@ int hlbm_batch_tune(hlbm_batch* b, int32_t variant) {
         return fail(HLBM_EPLAN, "hlbm_batch_tune: a member's rows do not suit the pipelined kernel");
   b->variant = variant;
   b->dirty = true;
+  return HLBM_OK;
+}
+
+// One timed replay per candidate: the batch's own launches (variants 6 - 9) or every member's own
+// kernel forked onto its stream (variant 10), each reading the current state and writing the idle
+// buffers, so no member's state advances (the zero-gradient outlet passes rewrite the same values).
+int hlbm_batch_autotune(hlbm_batch* b, int32_t reps, int32_t* chosen, double* ms_per_variant) {
+  if (!b || reps < 1) return fail(HLBM_EINVAL, "hlbm_batch_autotune: bad argument");
+  for (int v = 0; v < HLBM_BATCH_VARIANTS; v++)
+    if (ms_per_variant) ms_per_variant[v] = -1.0;
+  if (b->members.empty()) {
+    if (chosen) *chosen = b->variant;
+    return HLBM_OK;
+  }
+  HLBM_CK(cudaSetDevice(b->device));
+  for (hlbm_ctx* c : b->members) {
+    if (int rc = build_plan(c)) return rc;
+    if (c->phase == MATER) c->phase = POSTCOL;  // the state is the post-collision one either way
+    HLBM_CK(cudaStreamSynchronize(c->stream));
+  }
+  cudaEvent_t e0, e1;
+  HLBM_CK(cudaEventCreate(&e0));
+  HLBM_CK(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch) -> double {  // ms of one replay, after one untimed one
+    if (launch() != cudaSuccess) return -1.0;
+    if (cudaEventRecord(e0, b->stream) != cudaSuccess) return -1.0;
+    for (int r = 0; r < reps; r++)
+      if (launch() != cudaSuccess) return -1.0;
+    float ms = 0.0f;
+    if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return -1.0;
+    return double(ms) / reps;
+  };
+  const int saved = b->variant;
+  int best = saved;
+  double best_ms = 1e300;
+  int rc = HLBM_OK;
+  for (int v = 6; v <= 10 && rc == HLBM_OK; v++) {
+    double ms = -1.0;
+    if (v <= 9) {
+      bool fits = true;
+      if (v < 8)
+        for (hlbm_ctx* c : b->members) fits = fits && (size_t(c->n[0]) * elem_size(c->precision)) % 16 == 0;
+      if (!fits) continue;
+      b->variant = v;
+      b->dirty = true;
+      if (batch_rebuild(b) != HLBM_OK) continue;  // tiles do not fit this kernel's stages
+      b->descs_stale = true;
+      if ((rc = batch_refresh_descs(b)) != HLBM_OK) break;
+      ms = timed([&] { return batch_launch(b, 0); });
+    } else {
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      if (!b->fork_ev && cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) != cudaSuccess) continue;
+      cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) e = cudaEventRecord(b->fork_ev, b->stream);
+      for (hlbm_ctx* c : b->members) {
+        if (e == cudaSuccess && !c->join_ev) e = cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, b->fork_ev, 0);
+        if (e == cudaSuccess)
+          e = launch_with_plan(c, c->phase == RAW ? MODE_PROLOGUE : MODE_FUSED, c->f[c->cur], c->f[1 - c->cur],
+                               c->plan, concurrent_variant(c), c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->join_ev, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, c->join_ev, 0);
+      }
+      const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+      if (e == cudaSuccess && e2 == cudaSuccess && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess)
+        ms = timed([&] { return cudaGraphLaunch(exec, b->stream); });
+      if (exec) cudaGraphExecDestroy(exec);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+    }
+    if (ms_per_variant) ms_per_variant[v - 6] = ms;
+    if (ms > 0.0 && ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != HLBM_OK) {
+    b->variant = saved;
+    b->dirty = true;
+    return rc;
+  }
+  int e = 0;
+  HLBM_CK(cudaMemcpy(&e, b->err_dev, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(b->err_dev, 0, sizeof(int));
+    b->variant = saved;
+    b->dirty = true;
+    return fail(HLBM_ECUDA, "hlbm_batch_autotune: a shared-memory pipeline wait timed out");
+  }
+  b->variant = best;
+  b->dirty = true;  // tiles and graphs follow the chosen kernel at the next step
+  b->descs_stale = true;
+  if (chosen) *chosen = best;
   return HLBM_OK;
 }
 

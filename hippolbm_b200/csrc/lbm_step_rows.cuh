@@ -161,6 +161,40 @@ __device__ __forceinline__ void rows_read(const S* row, int x0, int nx, bool bou
   }
 }
 
+// rows_read for a group away from the row ends of a row that pulls from no bounced row: every
+// value is in the staged row, no test.
+template <typename S, int I>
+__device__ __forceinline__ void rows_read_interior(const S* row, int x0, uint32_t (&w)[2], float (&f)[4]) {
+  constexpr int ex = D3Q19::ex[I];
+  if constexpr (is_16bit<S>()) {
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(row);
+    const uint2 v = *reinterpret_cast<const uint2*>(words + x0 / 2);
+    if constexpr (ex == 0) {
+      w[0] = v.x;
+      w[1] = v.y;
+    } else if constexpr (ex == 1) {
+      const uint32_t lo = words[x0 / 2 - 1];
+      w[0] = __byte_perm(lo, v.x, 0x5432);
+      w[1] = __byte_perm(v.x, v.y, 0x5432);
+    } else {
+      const uint32_t hi = words[x0 / 2 + 2];
+      w[0] = __byte_perm(v.x, v.y, 0x5432);
+      w[1] = __byte_perm(v.y, hi, 0x5432);
+    }
+    (void)f;
+  } else {
+    const float4 v = *reinterpret_cast<const float4*>(row + x0);
+    if constexpr (ex == 0) {
+      f[0] = v.x, f[1] = v.y, f[2] = v.z, f[3] = v.w;
+    } else if constexpr (ex == 1) {
+      f[0] = row[x0 - 1], f[1] = v.x, f[2] = v.y, f[3] = v.z;
+    } else {
+      f[0] = v.y, f[1] = v.z, f[2] = v.w, f[3] = row[x0 + 4];
+    }
+    (void)w;
+  }
+}
+
 template <typename S, int COLL, int STAGES, int MINB>
 __global__ void __launch_bounds__(ROWS_THREADS, MINB)
     k_step_rows(const __grid_constant__ Planes<S> pl, const int8_t* __restrict__ flags, const StepPlan p,
@@ -250,12 +284,18 @@ __global__ void __launch_bounds__(ROWS_THREADS, MINB)
       const uint32_t fl4 = *reinterpret_cast<const uint32_t*>(sflags + size_t(r) * nx + x0);
       uint32_t words[Q][2];
       float vals[Q][4];
-      Unroll<0, Q>::run([&]<int I>() {
-        constexpr int ey = D3Q19::ey[I], ez = D3Q19::ez[I];
-        const bool bounced = (ey == 1 && oy0) || (ey == -1 && oyl) || (ez == 1 && oz0) || (ez == -1 && ozl);
-        rows_read<S, I>(st + size_t(I) * dir_elems + size_t(r) * nx, x0, nx, bounced, pl, own_row, p, words[I],
-                        vals[I]);
-      });
+      if (!(oy0 || oyl || oz0 || ozl) && x0 > 0 && x0 + ROWS_NODES_PER_THREAD < nx) {  // no bounce, no row end
+        Unroll<0, Q>::run([&]<int I>() {
+          rows_read_interior<S, I>(st + size_t(I) * dir_elems + size_t(r) * nx, x0, words[I], vals[I]);
+        });
+      } else {
+        Unroll<0, Q>::run([&]<int I>() {
+          constexpr int ey = D3Q19::ey[I], ez = D3Q19::ez[I];
+          const bool bounced = (ey == 1 && oy0) || (ey == -1 && oyl) || (ez == 1 && oz0) || (ez == -1 && ozl);
+          rows_read<S, I>(st + size_t(I) * dir_elems + size_t(r) * nx, x0, nx, bounced, pl, own_row, p, words[I],
+                          vals[I]);
+        });
+      }
       Unroll<0, 2>::run([&]<int J>() {
         const int8_t fa = int8_t(fl4 >> (16 * J)), fb = int8_t(fl4 >> (16 * J + 8));
         float2 v[Q];

@@ -203,7 +203,7 @@ int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
  * The FP32 and 16-bit tiers update node pairs in packed FP32 where a plan has no body force, no
  * start_iteration boxes and no wall nodes outside wall_bounce_back; other plans run one node per
  * thread.  A context starts at its tier's default (hlbm_autotune's pick on 512^3 Couette: FP64 4,
- * FP32 1, FP16 / BF16 5 with BGK and 3 with MRT) until hlbm_tune or hlbm_autotune chooses.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
+ * FP32 1, FP16 / BF16 8 with BGK and 9 with MRT) until hlbm_tune or hlbm_autotune chooses.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
  * into shared-memory stages (256 or 512 threads per CTA; needs nx * bytes per population to be a
  * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
  * variant on this lattice (from the current populations into the idle buffer, so the state does
@@ -249,6 +249,14 @@ int hlbm_batch_add(hlbm_batch* b, hlbm_ctx* lattice);
 int hlbm_batch_remove(hlbm_batch* b, hlbm_ctx* lattice);
 int hlbm_batch_step(hlbm_batch* b, int64_t nsteps);
 int hlbm_batch_tune(hlbm_batch* b, int32_t variant);
+/* The batch's kernel chosen by measurement (no reference counterpart): times `reps` replays of one
+ * step of every batch variant that applies (6, 7: pipelined kernel; 8, 9: tile-list kernel; 10:
+ * every member's own tuned kernel on its own stream) on the batch itself -- each reading the
+ * members' current state and writing their idle buffers, so no member advances -- keeps the fastest
+ * and returns it in *chosen and the per-variant times (ms per step, -1 if skipped) in
+ * ms_per_variant[HLBM_BATCH_VARIANTS], index variant - 6. */
+#define HLBM_BATCH_VARIANTS 5
+int hlbm_batch_autotune(hlbm_batch* b, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* info = {members, tiles, tile elements, stages, graph replays, kernel launches} */
 int hlbm_batch_info(hlbm_batch* b, int64_t info[6]);
 /* the batch's cudaStream_t (every batched launch is issued on it), as a pointer-sized handle */

@@ -182,3 +182,44 @@ def test_concurrent_members_equal_their_runs_alone(precision):
             f1 = one.populations()
             m = carried(case, one.flags())
         assert np.array_equal(f[:, m], f1[:, m]), case.name
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_batch_autotune_leaves_every_member_unchanged(precision):
+    """hlbm_batch_autotune times every batch kernel on the batch and keeps the fastest: no member's
+    state moves (also for members that have not stepped yet), and the batch then steps like a batch
+    tuned to that kernel by hand."""
+    from hippolbm_b200.batch import Batch
+    from hippolbm_b200.lattice import Lattice
+
+    lats = [Lattice.from_case(c, precision) for c in CASES]
+    with Batch(precision) as b:
+        for lat in lats:
+            b.add(lat)
+        b.step(3)
+        before = [lat.populations() for lat in lats]
+        fresh = Lattice.from_case(CASES[0], precision)  # joins now: it has not stepped yet
+        b.add(fresh)
+        fresh_before = fresh.populations()
+        chosen, ms = b.autotune(reps=2)
+        assert chosen in ms and set(ms) <= {6, 7, 8, 9, 10} and {8, 9, 10} <= set(ms)
+        assert all(t > 0 for t in ms.values())
+        for lat, f in zip(lats, before):
+            assert np.array_equal(lat.populations(), f)
+        assert np.array_equal(fresh.populations(), fresh_before)
+        b.step(4)
+        got = [lat.populations() for lat in lats + [fresh]]
+    ref_lats = [Lattice.from_case(c, precision) for c in CASES]
+    with Batch(precision) as r:  # the same calls with the chosen kernel set by hand
+        for lat in ref_lats:
+            r.add(lat)
+        r.step(3)
+        ref_fresh = Lattice.from_case(CASES[0], precision)
+        r.add(ref_fresh)
+        r.tune(chosen)
+        r.step(4)
+        want = [lat.populations() for lat in ref_lats + [ref_fresh]]
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+    for lat in lats + [fresh] + ref_lats + [ref_fresh]:
+        lat.close()
