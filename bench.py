@@ -46,8 +46,8 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_POP = {"f64": 8, "f64_strict": 8, "f32": 4, "f16": 2, "bf16": 2}
 DEFAULT_VARIANT = {("f64", "bgk"): 4, ("f64", "mrt"): 4, ("f64_strict", "bgk"): 4, ("f64_strict", "mrt"): 4,
-                   ("f32", "bgk"): 1, ("f32", "mrt"): 1, ("f16", "bgk"): 8, ("f16", "mrt"): 9,
-                   ("bf16", "bgk"): 8, ("bf16", "mrt"): 9}
+                   ("f32", "bgk"): 1, ("f32", "mrt"): 1, ("f16", "bgk"): 9, ("f16", "mrt"): 9,
+                   ("bf16", "bgk"): 9, ("bf16", "mrt"): 9}
 DTYPE = {"f64": "f64", "f64_strict": "f64", "f32": "f32", "f16": "f32 (f16 storage)", "bf16": "f32 (bf16 storage)"}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"

@@ -509,7 +509,8 @@ const char* hlbm_version(void) { return "hippolbm-b200 0.1.0 (sm_100a)"; }
 static int default_variant(int precision, int collision) {
   if (precision == HLBM_F64 || precision == HLBM_F64_STRICT) return 4;
   if (precision == HLBM_F32) return 1;
-  return collision == 1 ? 9 : 8;
+  (void)collision;
+  return 9;
 }
 
 int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double bmax[3], const int32_t periodic[3],

@@ -235,23 +235,23 @@ inline int rows_stages(const RowsGeometry& g, int ctas_per_sm) {
   return fit >= 4 ? 4 : int(fit);
 }
 
-template <typename S, int COLL, int STAGES, int MINB>
+template <typename S, int COLL, int STAGES, int WARPS, int MINB>
 cudaError_t launch_rows_t(const Planes<S>& pl, const int8_t* flags, const StepPlan& p, const RowsGeometry& g,
                           const TmaArgs& a, cudaStream_t s) {
-  auto kern = k_step_rows<S, COLL, STAGES, MINB>;
+  auto kern = k_step_rows<S, COLL, STAGES, WARPS, MINB>;
   const size_t smem = rows_smem_bytes(STAGES, g);
   if (cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) return e;
   const int grid = g.ntiles < a.sms * MINB ? g.ntiles : a.sms * MINB;
-  kern<<<grid, ROWS_THREADS, smem, s>>>(pl, flags, p, g, a.err, a.wait_limit);
+  kern<<<grid, 32 * (WARPS + 1), smem, s>>>(pl, flags, p, g, a.err, a.wait_limit);
   return cudaGetLastError();
 }
 
-template <typename S, int COLL, int MINB>
+template <typename S, int COLL, int WARPS, int MINB>
 cudaError_t launch_rows_stages(int stages, const Planes<S>& pl, const int8_t* flags, const StepPlan& p,
                                const RowsGeometry& g, const TmaArgs& a, cudaStream_t s) {
-  if (stages >= 4) return launch_rows_t<S, COLL, 4, MINB>(pl, flags, p, g, a, s);
-  if (stages == 3) return launch_rows_t<S, COLL, 3, MINB>(pl, flags, p, g, a, s);
-  return launch_rows_t<S, COLL, 2, MINB>(pl, flags, p, g, a, s);
+  if (stages >= 4) return launch_rows_t<S, COLL, 4, WARPS, MINB>(pl, flags, p, g, a, s);
+  if (stages == 3) return launch_rows_t<S, COLL, 3, WARPS, MINB>(pl, flags, p, g, a, s);
+  return launch_rows_t<S, COLL, 2, WARPS, MINB>(pl, flags, p, g, a, s);
 }
 
 template <typename S, typename R, bool STRICT>
@@ -260,21 +260,21 @@ cudaError_t launch_rows(int mode, int walls, const void* fin, void* fout, const 
   if constexpr (!is_16bit<S>()) {
     return cudaErrorNotSupported;
   } else {
-    if (mode != MODE_FUSED || !rows_eligible(p, int(sizeof(S)))) return cudaErrorNotSupported;
-    const RowsGeometry g = rows_geometry(p, int(sizeof(S)));
-    const int ctas = variant == 8 ? 2 : 1;
+    if (mode != MODE_FUSED || !rows_eligible(p, int(sizeof(S)), rows_warps(variant))) return cudaErrorNotSupported;
+    const int ctas = rows_ctas_per_sm(variant);
+    const RowsGeometry g = rows_geometry(p, int(sizeof(S)), rows_warps(variant));
     const int stages = rows_stages(g, ctas);
     if (stages < 2) return cudaErrorNotSupported;
     const S* fi = static_cast<const S*>(fin);
     S* fo = static_cast<S*>(fout);
     const Planes<S> pl = make_planes(fi, fo, p.stride);
     cudaError_t e;
-    if (ctas == 2)
-      e = p.collision == 0 ? launch_rows_stages<S, 0, 2>(stages, pl, flags, p, g, a, s)
-                           : launch_rows_stages<S, 1, 2>(stages, pl, flags, p, g, a, s);
+    if (variant == 8)
+      e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s)
+                           : launch_rows_stages<S, 1, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s);
     else
-      e = p.collision == 0 ? launch_rows_stages<S, 0, 1>(stages, pl, flags, p, g, a, s)
-                           : launch_rows_stages<S, 1, 1>(stages, pl, flags, p, g, a, s);
+      e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s)
+                           : launch_rows_stages<S, 1, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s);
     if (e) return e;
     if ((e = launch_faces<S, R, STRICT, MODE_FUSED, false>(fi, fo, flags, p, s))) return e;
     if (!walls) return cudaSuccess;
@@ -290,8 +290,8 @@ cudaError_t launch_rows(int mode, int walls, const void* fin, void* fout, const 
 // Whether a single-lattice launch of `variant` in `mode` runs the row pipeline; otherwise variants 8
 // and 9 run variant 5.
 inline bool rows_runs(const StepPlan& p, int variant, int mode, int bytes) {
-  if (variant < 8 || mode != MODE_FUSED || !rows_eligible(p, bytes)) return false;
-  return rows_stages(rows_geometry(p, bytes), variant == 8 ? 2 : 1) >= 2;
+  if (variant < 8 || mode != MODE_FUSED || !rows_eligible(p, bytes, rows_warps(variant))) return false;
+  return rows_stages(rows_geometry(p, bytes, rows_warps(variant)), rows_ctas_per_sm(variant)) >= 2;
 }
 
 template <typename S, typename R, bool STRICT>

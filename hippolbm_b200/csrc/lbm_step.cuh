@@ -862,27 +862,29 @@ __device__ __forceinline__ void plane_ops(R (&v)[Q], const S* __restrict__ fin, 
 // (macro_variables.hpp:56-69), else u = j.
 // feq_i / w_i - (sum v) = srho P_i is folded to two FMAs per direction: with eu = e_I.u for the
 // odd direction I, g_I = base + eu (s3 + s45 eu) and g_{I+1} = base + eu (s45 eu - s3).
-// The sums run over the opposite pairs: sum = v_0 + sum_p S_p and j_ax = sum_p e_{2p-1}[ax] D_p
-// in increasing p (the first term is p = ax + 1: directions 1, 3, 5, component +1).
+// The sums run over the opposite pairs: sum = v_0 + sum_p S_p and j_ax = sum_p e_{2p-1}[ax] D_p.
 template <typename V, bool DEVF>
 __device__ __forceinline__ void bgk_v(V (&v)[Q], const StepPlan& p) {
   using L = Lanes<V>;
   using T = typename L::S;
-  V sum = v[0], jx, jy, jz;
+  // opposite-pair sums S_p = f_{2p-1} + f_{2p} and differences D_p = f_{2p-1} - f_{2p}, reduced as
+  // balanced trees (depth 4 for the density, 3 for each momentum component) so the two lanes'
+  // chains leave the scheduler independent work
+  V S[10], D[10];
   Unroll<1, 10>::run([&]<int P>() {
-    constexpr int I = 2 * P - 1;
-    const V a = v[I], b = v[I + 1];
-    const V d = L::sub(a, b);
-    sum = L::add(sum, L::add(a, b));
-    auto acc = [&]<int C, int FIRST>(V& j) {
-      if constexpr (P == FIRST) j = d;
-      else if constexpr (C > 0) j = L::add(j, d);
-      else if constexpr (C < 0) j = L::sub(j, d);
-    };
-    acc.template operator()<D3Q19::ex[I], 1>(jx);
-    acc.template operator()<D3Q19::ey[I], 2>(jy);
-    acc.template operator()<D3Q19::ez[I], 3>(jz);
+    S[P] = L::add(v[2 * P - 1], v[2 * P]);
+    D[P] = L::sub(v[2 * P - 1], v[2 * P]);
   });
+  static_assert(D3Q19::ex[1] == 1 && D3Q19::ex[7] == 1 && D3Q19::ex[9] == 1 && D3Q19::ex[11] == 1 &&
+                    D3Q19::ex[13] == 1 && D3Q19::ey[3] == 1 && D3Q19::ey[7] == 1 && D3Q19::ey[9] == -1 &&
+                    D3Q19::ey[15] == 1 && D3Q19::ey[17] == 1 && D3Q19::ez[5] == 1 && D3Q19::ez[11] == 1 &&
+                    D3Q19::ez[13] == -1 && D3Q19::ez[15] == 1 && D3Q19::ez[17] == -1,
+                "momentum trees follow the D3Q19 direction order");
+  const V sum = L::add(L::add(L::add(v[0], S[1]), L::add(S[2], S[3])),
+                       L::add(L::add(L::add(S[4], S[5]), L::add(S[6], S[7])), L::add(S[8], S[9])));
+  const V jx = L::add(L::add(L::add(D[1], D[4]), L::add(D[5], D[6])), D[7]);
+  const V jy = L::sub(L::add(L::add(D[2], D[4]), L::add(D[8], D[9])), D[5]);
+  const V jz = L::sub(L::add(L::add(D[3], D[6]), D[8]), L::add(D[7], D[9]));
   V srho, cu;
   if constexpr (DEVF) {
     const V rho = L::fma(sum, L::splat(T(p.inv_scale)), L::splat(T(p.rho0)));

@@ -2,17 +2,19 @@
 // source rows into shared memory, node pairs updated from there in packed FP32.
 //
 // Work is a list of tiles, each `rows` consecutive x-rows (y0 .. y0 + rows - 1) of one z-plane,
-// about 1024 nodes.  Warp 0 of a CTA produces: for every tile of its share, lane I (< 19) issues
-// the cp.async.bulk copies of direction I's source rows (y - e_y, z - e_z; periodic images, or the
-// node's own plane opp(I) where the source lies outside a non-periodic face) into a stage, and lane
-// 19 copies the tile's flag bytes; all complete on the stage's `full` mbarrier.  Warps 1..8
-// consume: each thread takes four consecutive nodes of a row, reads every direction's values for
-// them from the stage -- the x-shift of a pull is an offset in the row (two aligned words and a
-// byte permute for e_x = +-1), the row ends wrap inside the row or, on a non-periodic x face,
-// bounce back with one global load -- collides the two node pairs in packed FP32, rounds them
-// (16-bit tiers: stochastic rounding into packed words) and stores straight to global memory with
-// one 8- or 16-byte store per direction.  STAGES tiles are in flight while the consumers compute,
-// so memory latency is off the consumers' path and few registers hold data.
+// at most 128 nodes per consumer warp.  Warp 0 of a CTA produces: for every tile of its share, lane
+// I (< 19) issues the cp.async.bulk copies of direction I's source rows (y - e_y, z - e_z; periodic
+// images, or the node's own plane opp(I) where the source lies outside a non-periodic face) into a
+// stage, and lane 19 copies the tile's flag bytes; all complete on the stage's `full` mbarrier.
+// The other warps consume: each thread takes four consecutive nodes of a row (the same row and
+// columns in every tile), reads every direction's values for them from the stage -- one base
+// address with a compile-time offset per direction; the x-shift of a pull is an offset in the row
+// (two aligned words and a byte permute for e_x = +-1), the row ends wrap inside the row or, on a
+// non-periodic x face, bounce back with one global load -- and releases the stage at once (the
+// producer refills it while the collisions run).  It then collides the two node pairs in packed
+// FP32, rounds them (16-bit tiers: stochastic rounding into packed words) and stores straight to
+// global memory with one 8- or 16-byte store per direction.  STAGES tiles are in flight while the
+// consumers compute, so memory latency is off the consumers' path and few registers hold data.
 //
 // Like the vectorised kernel it applies no boundary operator (the face pass follows) and no wall
 // test (the wall fix-up follows on lattices with wall obstacles), and takes fused steps only.
@@ -25,34 +27,43 @@
 
 namespace hlbm {
 
-constexpr int ROWS_CONSUMER_WARPS = 8;
-constexpr int ROWS_THREADS = 32 * (ROWS_CONSUMER_WARPS + 1);  // warp 0 produces
-constexpr int ROWS_NODES_PER_THREAD = 4;                        // two node pairs
-constexpr int ROWS_TILE_NODES = ROWS_CONSUMER_WARPS * 32 * ROWS_NODES_PER_THREAD;
+constexpr int ROWS_NODES_PER_THREAD = 4;  // two node pairs
+
+// Consumer warps and CTAs per SM of the two variants (each CTA adds its producer warp):
+// variant 8 runs two CTAs of 8 consumer warps per SM (96 registers a thread), variant 9 one CTA of
+// 12 (128 registers a thread: 13 warps leave 4 per scheduler).  The register budget decides: the
+// node-pair collision of 38 lanes of state plus the other pair's 19 staged words spills heavily
+// at 96 registers, and 12 warps at 128 registers step a 512^3 lattice 1.1x (BGK) to 1.2x (MRT)
+// faster than 16 at 96.
+constexpr int rows_warps(int variant) { return variant == 8 ? 8 : 12; }
+constexpr int rows_ctas_per_sm(int variant) { return variant == 8 ? 2 : 1; }
+constexpr int rows_tile_nodes(int warps) { return warps * 32 * ROWS_NODES_PER_THREAD; }
 
 // Geometry of the row pipeline for one lattice: `rows` per tile, stage bytes, tiles.
 struct RowsGeometry {
   int rows = 0;
   int tiles_per_plane = 0;
   int ntiles = 0;
-  size_t stage_bytes = 0;  // 19 direction blocks of rows * nx values, then rows * nx flag bytes
+  size_t stage_bytes = 0;  // 19 direction blocks of tile-node values (rows * nx used), then the flag bytes
 };
 
 inline size_t rows_align128(size_t b) { return (b + 127) / 128 * 128; }
 
 // Whether a lattice can take the row pipeline: a 16-bit tier, rows of whole 16-byte chunks of flag
-// bytes (and so of populations), 32-bit node offsets, and the pair kernels' plan conditions.
-inline bool rows_eligible(const StepPlan& p, int bytes) {
-  return bytes == 2 && p.nx % 16 == 0 && p.ncell <= int64_t(0xffffffffu) && pair_kernels_apply(p, bytes);
+// bytes (and so of populations) and no longer than a tile, 32-bit node offsets, and the pair
+// kernels' plan conditions.
+inline bool rows_eligible(const StepPlan& p, int bytes, int warps) {
+  return bytes == 2 && p.nx % 16 == 0 && p.nx <= rows_tile_nodes(warps) && p.ncell <= int64_t(0xffffffffu) &&
+         pair_kernels_apply(p, bytes);
 }
 
-inline RowsGeometry rows_geometry(const StepPlan& p, int bytes) {
+inline RowsGeometry rows_geometry(const StepPlan& p, int bytes, int warps) {
   RowsGeometry g;
-  g.rows = ROWS_TILE_NODES / p.nx > 0 ? ROWS_TILE_NODES / p.nx : 1;
+  g.rows = rows_tile_nodes(warps) / p.nx > 0 ? rows_tile_nodes(warps) / p.nx : 1;
   if (g.rows > p.ny) g.rows = p.ny;
   g.tiles_per_plane = (p.ny + g.rows - 1) / g.rows;
   g.ntiles = g.tiles_per_plane * p.nz;
-  g.stage_bytes = rows_align128(size_t(Q) * g.rows * p.nx * bytes + size_t(g.rows) * p.nx);
+  g.stage_bytes = rows_align128(size_t(Q + 1) * rows_tile_nodes(warps) * bytes);
   return g;
 }
 
@@ -195,8 +206,8 @@ __device__ __forceinline__ void rows_read_interior(const S* row, int x0, uint32_
   }
 }
 
-template <typename S, int COLL, int STAGES, int MINB>
-__global__ void __launch_bounds__(ROWS_THREADS, MINB)
+template <typename S, int COLL, int STAGES, int WARPS, int MINB>
+__global__ void __launch_bounds__(32 * (WARPS + 1), MINB)
     k_step_rows(const __grid_constant__ Planes<S> pl, const int8_t* __restrict__ flags, const StepPlan p,
                 RowsGeometry g, int* __restrict__ err, long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -205,12 +216,14 @@ __global__ void __launch_bounds__(ROWS_THREADS, MINB)
   unsigned char* stages = smem_raw + 128;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nx = p.nx;
-  const size_t dir_elems = size_t(g.rows) * nx;
+  // direction I's rows start at element I * TILE of a stage (an immediate offset from one base);
+  // the tile's flag bytes follow the 19 blocks
+  constexpr int TILE = rows_tile_nodes(WARPS);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], ROWS_CONSUMER_WARPS);
+      mbar_init(&empty[s], WARPS);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -232,10 +245,10 @@ __global__ void __launch_bounds__(ROWS_THREADS, MINB)
         mbar_arrive_expect_tx(&full[s], unsigned(size_t(Q) * rows * nx * sizeof(S) + size_t(rows) * nx));
       __syncwarp();
       if (lane < Q) {
-        rows_issue_direction<S>(pl, p, z, y0, rows, reinterpret_cast<S*>(st) + size_t(lane) * dir_elems, &full[s],
+        rows_issue_direction<S>(pl, p, z, y0, rows, reinterpret_cast<S*>(st) + lane * TILE, &full[s],
                                 lane);
       } else if (lane == Q) {
-        bulk_copy(st + size_t(Q) * dir_elems * sizeof(S), flags + (uint32_t(z) * uint32_t(p.ny) + uint32_t(y0)) * nx,
+        bulk_copy(st + Q * TILE * sizeof(S), flags + (uint32_t(z) * uint32_t(p.ny) + uint32_t(y0)) * nx,
                   unsigned(rows * nx), &full[s]);
       }
     }
@@ -248,10 +261,12 @@ __global__ void __launch_bounds__(ROWS_THREADS, MINB)
 
   // ------------------------------------------------------------------------ consumers
   const int ctid = threadIdx.x - 32;
-  constexpr int NC = 32 * ROWS_CONSUMER_WARPS;
   const uint32_t seed = launch_seed<S>(p);
+  // nx <= TILE, so a tile's groups of four nodes (rows * nx / 4 <= TILE / 4) are at most one per
+  // consumer thread, and a thread takes the same row and columns of every tile
   const int groups_per_row = nx / ROWS_NODES_PER_THREAD;
-  const float inv_gpr = 1.0f / float(groups_per_row);
+  const int r = ctid / groups_per_row;
+  const int x0 = (ctid - r * groups_per_row) * ROWS_NODES_PER_THREAD;
   const bool sr = is_16bit<S>() && p.rounding;
   int k = 0;
   for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x, k++) {
@@ -263,70 +278,65 @@ __global__ void __launch_bounds__(ROWS_THREADS, MINB)
     const int z = t / g.tiles_per_plane, y0 = (t - z * g.tiles_per_plane) * g.rows;
     const int rows = (p.ny - y0) < g.rows ? (p.ny - y0) : g.rows;
     const S* st = reinterpret_cast<const S*>(stages + size_t(s) * g.stage_bytes);
-    const int8_t* sflags = reinterpret_cast<const int8_t*>(st + size_t(Q) * dir_elems);
-    for (int gi = ctid; gi < rows * groups_per_row; gi += NC) {
-      int r = __float2int_rz(float(gi) * inv_gpr);  // gi / groups_per_row, exact after one correction
-      int gx = gi - r * groups_per_row;
-      if (gx < 0) {
-        r--;
-        gx += groups_per_row;
-      } else if (gx >= groups_per_row) {
-        r++;
-        gx -= groups_per_row;
-      }
-      const int x0 = gx * ROWS_NODES_PER_THREAD;
-      const int y = y0 + r;
-      const uint32_t own_row = (uint32_t(z) * uint32_t(p.ny) + uint32_t(y)) * uint32_t(nx);
-      const uint32_t own = own_row + uint32_t(x0);
-      // the directions whose source row lies outside a non-periodic y / z face (bounced rows)
-      const bool oy0 = !p.periodic[1] && y == 0, oyl = !p.periodic[1] && y == p.ny - 1;
-      const bool oz0 = !p.periodic[2] && z == 0, ozl = !p.periodic[2] && z == p.nz - 1;
-      const uint32_t fl4 = *reinterpret_cast<const uint32_t*>(sflags + size_t(r) * nx + x0);
-      uint32_t words[Q][2];
-      float vals[Q][4];
+    const int8_t* sflags = reinterpret_cast<const int8_t*>(st + Q * TILE);
+    const bool active = r < rows;
+    const int y = y0 + r;
+    const uint32_t own_row = (uint32_t(z) * uint32_t(p.ny) + uint32_t(y)) * uint32_t(nx);
+    const uint32_t own = own_row + uint32_t(x0);
+    // the directions whose source row lies outside a non-periodic y / z face (bounced rows)
+    const bool oy0 = !p.periodic[1] && y == 0, oyl = !p.periodic[1] && y == p.ny - 1;
+    const bool oz0 = !p.periodic[2] && z == 0, ozl = !p.periodic[2] && z == p.nz - 1;
+    uint32_t fl4 = 0;
+    uint32_t words[Q][2];
+    float vals[Q][4];
+    if (active) {
+      fl4 = *reinterpret_cast<const uint32_t*>(sflags + size_t(r) * nx + x0);
       if (!(oy0 || oyl || oz0 || ozl) && x0 > 0 && x0 + ROWS_NODES_PER_THREAD < nx) {  // no bounce, no row end
         Unroll<0, Q>::run([&]<int I>() {
-          rows_read_interior<S, I>(st + size_t(I) * dir_elems + size_t(r) * nx, x0, words[I], vals[I]);
+          rows_read_interior<S, I>(st + I * TILE + r * nx, x0, words[I], vals[I]);
         });
       } else {
         Unroll<0, Q>::run([&]<int I>() {
           constexpr int ey = D3Q19::ey[I], ez = D3Q19::ez[I];
           const bool bounced = (ey == 1 && oy0) || (ey == -1 && oyl) || (ez == 1 && oz0) || (ez == -1 && ozl);
-          rows_read<S, I>(st + size_t(I) * dir_elems + size_t(r) * nx, x0, nx, bounced, pl, own_row, p, words[I],
+          rows_read<S, I>(st + I * TILE + r * nx, x0, nx, bounced, pl, own_row, p, words[I],
                           vals[I]);
         });
       }
-      Unroll<0, 2>::run([&]<int J>() {
-        const int8_t fa = int8_t(fl4 >> (16 * J)), fb = int8_t(fl4 >> (16 * J + 8));
-        float2 v[Q];
-        if constexpr (is_16bit<S>())
-          Unroll<0, Q>::run([&]<int I>() { v[I] = unpack2<S>(words[I][J]); });
-        else
-          Unroll<0, Q>::run([&]<int I>() { v[I] = make_float2(vals[I][2 * J], vals[I][2 * J + 1]); });
-        pair_update<S, MODE_FUSED, COLL>(v, p, fa, fb);
-        if constexpr (is_16bit<S>()) {
-          uint32_t h = 0, h2 = 0;
-          if (sr) {
-            h = node_hash(int64_t(own) + 2 * J, seed);
-            h2 = second_hash(h);
-          }
-          pack_pair<S>(v, sr, h, h2, [&]<int I>(uint32_t w) { words[I][J] = w; });
-        } else {
-          Unroll<0, Q>::run([&]<int I>() {
-            vals[I][2 * J] = v[I].x;
-            vals[I][2 * J + 1] = v[I].y;
-          });
-        }
-      });
-      if constexpr (is_16bit<S>())
-        Unroll<0, Q>::run([&]<int I>() { *reinterpret_cast<uint2*>(pl.out[I] + own) = make_uint2(words[I][0], words[I][1]); });
-      else
-        Unroll<0, Q>::run([&]<int I>() {
-          *reinterpret_cast<float4*>(pl.out[I] + own) = make_float4(vals[I][0], vals[I][1], vals[I][2], vals[I][3]);
-        });
     }
+    // every value this warp reads from the stage is in registers: release it, so the producer
+    // refills it while the collisions run rather than after them
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (!active) continue;
+    Unroll<0, 2>::run([&]<int J>() {
+      const int8_t fa = int8_t(fl4 >> (16 * J)), fb = int8_t(fl4 >> (16 * J + 8));
+      float2 v[Q];
+      if constexpr (is_16bit<S>())
+        Unroll<0, Q>::run([&]<int I>() { v[I] = unpack2<S>(words[I][J]); });
+      else
+        Unroll<0, Q>::run([&]<int I>() { v[I] = make_float2(vals[I][2 * J], vals[I][2 * J + 1]); });
+      pair_update<S, MODE_FUSED, COLL>(v, p, fa, fb);
+      if constexpr (is_16bit<S>()) {
+        uint32_t h = 0, h2 = 0;
+        if (sr) {
+          h = node_hash(int64_t(own) + 2 * J, seed);
+          h2 = second_hash(h);
+        }
+        pack_pair<S>(v, sr, h, h2, [&]<int I>(uint32_t w) { words[I][J] = w; });
+      } else {
+        Unroll<0, Q>::run([&]<int I>() {
+          vals[I][2 * J] = v[I].x;
+          vals[I][2 * J + 1] = v[I].y;
+        });
+      }
+    });
+    if constexpr (is_16bit<S>())
+      Unroll<0, Q>::run([&]<int I>() { *reinterpret_cast<uint2*>(pl.out[I] + own) = make_uint2(words[I][0], words[I][1]); });
+    else
+      Unroll<0, Q>::run([&]<int I>() {
+        *reinterpret_cast<float4*>(pl.out[I] + own) = make_float4(vals[I][0], vals[I][1], vals[I][2], vals[I][3]);
+      });
   }
 }
 

@@ -50,7 +50,7 @@ __device__ __forceinline__ void advance_step_numbers(LatticeDesc* lats, int ndes
 // tile: {lattice, z, y0, rows}
 using Tile = int4;
 
-constexpr long long TMA_WAIT_LIMIT = 20000000;  // ~1 s of polling before a wait gives up
+constexpr long long TMA_WAIT_LIMIT = 20000000;  // polls before a wait gives up (and at most ~2 s)
 constexpr int TMA_ERR_TIMEOUT = 1;
 
 // direction components for loops indexed at run time: 2 bits per direction (component + 1)
@@ -80,20 +80,39 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
                : "memory");
 }
 
-// polls the phase with the given parity; false if it did not complete within `limit` polls
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase with the given parity; false if it did not complete within `limit` polls or
+// about two seconds.  The first poll is a non-blocking test; the others are `try_wait`, which
+// suspends the thread in hardware until the phase completes or about a microsecond passes, so a
+// waiting warp takes no issue slots from the warps that compute.
+constexpr unsigned long long MBAR_WAIT_NS = 2000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit = TMA_WAIT_LIMIT) {
   const unsigned a = smem_addr(bar);
-  for (long long it = 0; it < limit; it++) {
-    unsigned done;
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  if (done) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long it = 1; it < limit; it++) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(1000u)
         : "memory");
     if (done) return true;
-    if (it > 64) __nanosleep(32);
+    if ((it & 63) == 0 && global_ns() - t0 > MBAR_WAIT_NS) return false;
   }
   return false;
 }

@@ -203,16 +203,17 @@ int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
  * The FP32 and 16-bit tiers update node pairs in packed FP32 where a plan has no body force, no
  * start_iteration boxes and no wall nodes outside wall_bounce_back; other plans run one node per
  * thread.  A context starts at its tier's default (hlbm_autotune's pick on 512^3 Couette: FP64 4,
- * FP32 1, FP16 / BF16 8 with BGK and 9 with MRT) until hlbm_tune or hlbm_autotune chooses.  Variants 6, 7: persistent kernel fed by bulk asynchronous copies of whole rows
+ * FP32 1, FP16 / BF16 9) until hlbm_tune or hlbm_autotune chooses.  Variants 6, 7: persistent
+ * kernel fed by bulk asynchronous copies of whole rows
  * into shared-memory stages (256 or 512 threads per CTA; needs nx * bytes per population to be a
  * multiple of 16; otherwise variant 4 runs).  hlbm_autotune times `reps` fused launches of every
  * variant on this lattice (from the current populations into the idle buffer, so the state does
  * not advance), keeps the fastest, and returns it in *chosen and the per-variant times (ms, -1 if
  * skipped) in ms_per_variant[HLBM_NUM_VARIANTS].  Variants 8, 9 (FP16 / BF16): the row pipeline --
- * a producer warp bulk-copies each tile's source rows and flags into shared-memory stages, eight
- * consumer warps update node pairs from there in packed FP32 -- with two (8) or one (9) CTA per
- * SM; fused steps of lattices with nx % 16 == 0 and the pair kernels' plan conditions, else
- * variant 5 runs. */
+ * a producer warp bulk-copies each tile's source rows and flags into shared-memory stages,
+ * consumer warps update node pairs from there in packed FP32 -- with two CTAs of 8 consumer warps
+ * (8) or one CTA of 12 (9) per SM; fused steps of lattices with nx % 16 == 0, nx <= 1024 (8) or
+ * 1536 (9) and the pair kernels' plan conditions, else variant 5 runs. */
 #define HLBM_NUM_VARIANTS 10
 int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);

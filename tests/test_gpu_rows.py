@@ -3,8 +3,8 @@ memory, node pairs updated from there) gives the same populations as the pair ke
 bit for bit and with stochastic rounding on: both update the same node pairs with the same packed
 FP32 arithmetic and round them with the same random bits.  The cases cover periodic and bounced
 x ends, bounced y / z rows, tiles of one and of several rows, a tile that wraps a periodic y edge,
-boundary operators on every face kind (face pass), wall obstacles (wall fix-up) and both
-collisions."""
+boundary operators on every face kind (face pass), wall obstacles (wall fix-up), both collisions,
+and rows longer than a tile (the vectorised kernel runs instead)."""
 import numpy as np
 import pytest
 
@@ -26,6 +26,15 @@ def cases():
                                                                       "regions": ["plan_xy_l"]}),
                                              Op("neumann", {"U": [0.0, 0.0, 0.0], "regions": ["plan_yz_0"]})],
                         steps=12))
+    # rows longer than a tile of variant 8 (1024 nodes) but not of variant 9 (1536), and longer than
+    # both: variant 8 (and then 9) runs the vectorised kernel instead
+    out.append(Case(name="long_rows_1088", cell_dims=(1087, 5, 4), bmin=(0, 0, 0), bmax=(1087, 5, 4),
+                    periodic=(True, True, False), tau=0.7, nuth=0.1, collision="bgk",
+                    pre_stream_bcs=[Op("pre_bounce_back")], post_stream_bcs=[Op("post_bounce_back")],
+                    boundary_conditions=[Op("lid_driven_cavity", {"U": [0.05, 0.0, 0.0], "regions": ["plan_xy_l"]})],
+                    steps=12))
+    out.append(Case(name="long_rows_1600", cell_dims=(1599, 3, 2), bmin=(0, 0, 0), bmax=(1599, 3, 2),
+                    periodic=(True, True, True), tau=0.7, nuth=0.1, collision="mrt", steps=12))
     return out
 
 
