@@ -219,8 +219,10 @@ int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
 /* the context's cudaStream_t, as a pointer-sized handle */
 void* hlbm_stream(hlbm_ctx* ctx);
-/* Bound on each wait of the pipelined kernel (variants 6, 7) in polls of its shared-memory
- * barrier; 0 restores the default of about a second.  No reference counterpart.  A wait that runs
+/* Bound on each wait of the pipelined kernels (variants 6 - 9) in polls of their shared-memory
+ * barriers (the first poll a test, the others a hardware-suspended try_wait of up to about a
+ * microsecond); 0 restores the default of 2e7 polls.  Every wait also gives up after two seconds
+ * whatever the bound.  No reference counterpart.  A wait that runs
  * out records an error on the device and its CTA returns after its copies in flight have landed;
  * the next call that reads the state (hlbm_get_populations, hlbm_simulation_state, ...) fails with
  * HLBM_ECUDA and clears the record, and the context stays usable (put populations back and step
