@@ -564,7 +564,9 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
     cudaGetLastError();
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate the error word"));
   }
-  if (pool_alloc((void**)&c->flags, size_t(c->ncell), c->device, c->stream) != cudaSuccess ||
+  // the flag bytes are padded to 128 (the span pipeline bulk-copies whole 16-byte chunks of them)
+  const size_t flag_bytes = size_t((c->ncell + 127) / 128 * 128);
+  if (pool_alloc((void**)&c->flags, flag_bytes, c->device, c->stream) != cudaSuccess ||
       pool_alloc((void**)&c->nearwall, size_t(c->ncell), c->device, c->stream) != cudaSuccess ||
       pool_alloc((void**)&c->partials, sizeof(double) * 4 * 148 * 8, c->device, c->stream) != cudaSuccess ||
       pool_alloc((void**)&c->stats_dev, sizeof(double) * 4, c->device, c->stream) != cudaSuccess) {
@@ -572,7 +574,7 @@ int hlbm_domain(const int32_t cell_dims[3], const double bmin[3], const double b
     return cleanup(fail(HLBM_ENOMEM, "hlbm_domain: cannot allocate flags"));
   }
   // init_obst: every flag FLUIDE_ (-1 = 0xff)
-  if (cudaMemsetAsync(c->flags, 0xff, size_t(c->ncell), c->stream) != cudaSuccess ||
+  if (cudaMemsetAsync(c->flags, 0xff, flag_bytes, c->stream) != cudaSuccess ||
       cudaMemsetAsync(c->nearwall, 0, size_t(c->ncell), c->stream) != cudaSuccess)
     return cleanup(fail(HLBM_ECUDA, "cudaMemsetAsync failed"));
   // default lbm_parameters slots (lbm_parameters.cpp:57-64)

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "lbm_step_rows.cuh"
+#include "lbm_step_spans.cuh"
 #include "lbm_step_tiles.cuh"
 #include "lbm_step_tma.cuh"
 #include "lbm_step_vec.cuh"
@@ -254,27 +255,69 @@ cudaError_t launch_rows_stages(int stages, const Planes<S>& pl, const int8_t* fl
   return launch_rows_t<S, COLL, 2, WARPS, MINB>(pl, flags, p, g, a, s);
 }
 
+// The span pipeline (lbm_step_spans.cuh) with the shape of variant 8 or 9; its stage count is the
+// one the variant's stage size allows (3 stages of 60 KB at one CTA per SM, 2 of 40 KB at two).
+constexpr size_t spans_stage_bytes(int warps) {
+  return (size_t(Q) * (spans_tile_nodes(warps) + 8) * 2 + size_t(spans_tile_nodes(warps)) + 127) / 128 * 128;
+}
+constexpr int spans_stage_count(int variant) {
+  const size_t budget = size_t(227 * 1024) / size_t(rows_ctas_per_sm(variant)) - 1024;
+  const size_t fit = (budget - 128) / spans_stage_bytes(rows_warps(variant));
+  return fit >= 4 ? 4 : int(fit);
+}
+static_assert(spans_stage_count(8) >= 2 && spans_stage_count(9) >= 2, "span pipeline stages must fit");
+
+template <typename S, int COLL, int VARIANT>
+cudaError_t launch_spans_t(const Planes<S>& pl, const int8_t* flags, const StepPlan& p, const SpansGeometry& g,
+                           const TmaArgs& a, cudaStream_t s) {
+  constexpr int WARPS = rows_warps(VARIANT), MINB = rows_ctas_per_sm(VARIANT), STAGES = spans_stage_count(VARIANT);
+  auto kern = k_step_spans<S, COLL, STAGES, WARPS, MINB>;
+  const size_t smem = spans_smem_bytes(STAGES, g);
+  if (cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) return e;
+  const int grid = g.ntiles < a.sms * MINB ? g.ntiles : a.sms * MINB;
+  kern<<<grid, 32 * (WARPS + 1), smem, s>>>(pl, flags, p, g, a.err, a.wait_limit);
+  return cudaGetLastError();
+}
+
+// Which pipeline a fused step of `variant` (8 or 9) runs on the lattice: 1 the row pipeline (rows
+// of whole 16-byte chunks), 2 the span pipeline (any other row length), 0 neither.
+inline int pipeline_kind(const StepPlan& p, int variant, int bytes) {
+  if (rows_eligible(p, bytes, rows_warps(variant)) &&
+      rows_stages(rows_geometry(p, bytes, rows_warps(variant)), rows_ctas_per_sm(variant)) >= 2)
+    return 1;
+  if (spans_eligible(p, bytes)) return 2;
+  return 0;
+}
+
 template <typename S, typename R, bool STRICT>
 cudaError_t launch_rows(int mode, int walls, const void* fin, void* fout, const int8_t* flags, const StepPlan& p,
                         cudaStream_t s, int variant, const TmaArgs& a) {
   if constexpr (!is_16bit<S>()) {
     return cudaErrorNotSupported;
   } else {
-    if (mode != MODE_FUSED || !rows_eligible(p, int(sizeof(S)), rows_warps(variant))) return cudaErrorNotSupported;
-    const int ctas = rows_ctas_per_sm(variant);
-    const RowsGeometry g = rows_geometry(p, int(sizeof(S)), rows_warps(variant));
-    const int stages = rows_stages(g, ctas);
-    if (stages < 2) return cudaErrorNotSupported;
+    const int kind = mode == MODE_FUSED ? pipeline_kind(p, variant, int(sizeof(S))) : 0;
+    if (kind == 0) return cudaErrorNotSupported;
     const S* fi = static_cast<const S*>(fin);
     S* fo = static_cast<S*>(fout);
     const Planes<S> pl = make_planes(fi, fo, p.stride);
     cudaError_t e;
-    if (variant == 8)
-      e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s)
-                           : launch_rows_stages<S, 1, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s);
-    else
-      e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s)
-                           : launch_rows_stages<S, 1, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s);
+    if (kind == 1) {
+      const int ctas = rows_ctas_per_sm(variant);
+      const RowsGeometry g = rows_geometry(p, int(sizeof(S)), rows_warps(variant));
+      const int stages = rows_stages(g, ctas);
+      if (variant == 8)
+        e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s)
+                             : launch_rows_stages<S, 1, rows_warps(8), rows_ctas_per_sm(8)>(stages, pl, flags, p, g, a, s);
+      else
+        e = p.collision == 0 ? launch_rows_stages<S, 0, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s)
+                             : launch_rows_stages<S, 1, rows_warps(9), rows_ctas_per_sm(9)>(stages, pl, flags, p, g, a, s);
+    } else {
+      const SpansGeometry g = spans_geometry(p, rows_warps(variant));
+      if (variant == 8)
+        e = p.collision == 0 ? launch_spans_t<S, 0, 8>(pl, flags, p, g, a, s) : launch_spans_t<S, 1, 8>(pl, flags, p, g, a, s);
+      else
+        e = p.collision == 0 ? launch_spans_t<S, 0, 9>(pl, flags, p, g, a, s) : launch_spans_t<S, 1, 9>(pl, flags, p, g, a, s);
+    }
     if (e) return e;
     if ((e = launch_faces<S, R, STRICT, MODE_FUSED, false>(fi, fo, flags, p, s))) return e;
     if (!walls) return cudaSuccess;
@@ -287,11 +330,10 @@ cudaError_t launch_rows(int mode, int walls, const void* fin, void* fout, const 
   }
 }
 
-// Whether a single-lattice launch of `variant` in `mode` runs the row pipeline; otherwise variants 8
-// and 9 run variant 5.
+// Whether a single-lattice launch of `variant` in `mode` runs the row or span pipeline; otherwise
+// variants 8 and 9 run variant 5.
 inline bool rows_runs(const StepPlan& p, int variant, int mode, int bytes) {
-  if (variant < 8 || mode != MODE_FUSED || !rows_eligible(p, bytes, rows_warps(variant))) return false;
-  return rows_stages(rows_geometry(p, bytes, rows_warps(variant)), rows_ctas_per_sm(variant)) >= 2;
+  return variant >= 8 && mode == MODE_FUSED && pipeline_kind(p, variant, bytes) != 0;
 }
 
 template <typename S, typename R, bool STRICT>

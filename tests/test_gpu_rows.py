@@ -17,7 +17,9 @@ def cases():
     out = []
     for coll in ("bgk", "mrt"):
         out.append(couette_case(64, tau=0.7, u_wall=0.05, steps=12, collision=coll))
-        c = sphere_channel_case((96, 40, 36), (30.0, 20.0, 18.0), 5.0, tau=0.6, u_in=0.02, steps=12, collision=coll)
+        # an even z-plane (97 x 42) with MRT: the reference variant 4 is then the pair kernel
+        c = sphere_channel_case((96, 41 if coll == "mrt" else 40, 36), (30.0, 20.0, 18.0), 5.0, tau=0.6, u_in=0.02,
+                                steps=12, collision=coll)
         out.append(c)
         out.append(Case(name=f"lid_{coll}", cell_dims=(31, 29, 27), bmin=(0, 0, 0), bmax=(31, 29, 27),
                         periodic=(False, True, False), tau=0.8, nuth=0.1, collision=coll,
