@@ -72,7 +72,7 @@ def parse_args():
     ap.add_argument("--autotune", action="store_true", help="time every variant on the lattice and keep the fastest")
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="16-bit storage rounding")
-    ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve", "parity"])
+    ap.add_argument("--workload", default="couette", choices=["couette", "precision", "batch", "serve", "parity", "solve"])
     ap.add_argument("--parity-steps", type=int, default=500, help="parity workload: time steps")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="precision workload: linear scale of the 1024x256x256 channel (steps scale alike)")
@@ -95,6 +95,9 @@ def parse_args():
     ap.add_argument("--serve-requests", type=int, default=16, help="default workload: requests of the serve summary")
     ap.add_argument("--serve-rate", type=float, default=100.0, help="default workload: arrival rate (req/s) of it")
     ap.add_argument("--rates", default="10,100,1000", help="serve workload: arrival rates (req/s)")
+    ap.add_argument("--solve", default="channel", choices=["cavity", "channel", "sphere"],
+                    help="solve workload: the kind of serving solve stepped alone")
+    ap.add_argument("--edges", default="181,150,170", help="solve workload: nodes along x, y, z")
     return ap.parse_args()
 
 
@@ -573,6 +576,46 @@ def run_serve(a):
     return 0
 
 
+def run_solve(a):
+    """One solve of the serving mix (--solve, --edges: every face non-periodic, the operators of
+    serve.solve_case) stepped alone at FP64 (variant 4) and at FP16 storage (the pair kernel,
+    variant 4, and the row / span pipeline, variant 9): W warm-up steps, K steps timed by CUDA
+    events on the lattice's stream, for each."""
+    import numpy as np
+    import torch
+
+    from hippolbm_b200 import serve
+    from hippolbm_b200.lattice import Lattice
+
+    edges = tuple(int(e) for e in a.edges.split(","))
+    case = serve.solve_case(a.solve, edges, a.tau, np.random.default_rng(20261203))
+    peak, peak_kind = measured_hbm_peak()
+    out = []
+    for precision, variant in (("f64", 4), ("f16", 4), ("f16", 9)):
+        with Lattice.from_case(case, precision) as lat:
+            lat.tune(variant)
+            stream = torch.cuda.ExternalStream(lat.stream_handle(), device=torch.device("cuda", 0))
+            lat.step(a.warmup)
+            lat.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lat.step(a.steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / a.steps
+            nodes = lat.ncell
+        alg = 38 * BYTES_PER_POP[precision] + 1
+        out.append({"precision": precision, "variant": variant, "ms_per_step": round(ms, 4),
+                    "mlups": round(nodes / (ms * 1e-3) / 1e6, 1),
+                    "frac": round(nodes * alg / (ms * 1e-3) / 1e9 / peak, 4)})
+    line = {"workload": "solve", "metric": "MLUPS", "value": out[-1]["mlups"], "unit": "MLUPS", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": f"{a.solve}_{edges[0]}x{edges[1]}x{edges[2]}", "tau": a.tau},
+            "frac_of": f"{peak_kind} copy bandwidth {peak} GB/s", "by_tier": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_parity(a):
     """The Couette workload (--n, --collision, --tau) on the CPU oracle and on the GPU in strict FP64
     and FP64: strict FP64 must equal the oracle in every population, FP64 stay within 1e-12 of it
@@ -627,6 +670,8 @@ def main():
         return run_serve(a)
     if a.workload == "parity":
         return run_parity(a)
+    if a.workload == "solve":
+        return run_solve(a)
     return run_ours(a)
 
 

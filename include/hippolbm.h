@@ -213,7 +213,10 @@ int hlbm_info(hlbm_ctx* ctx, int64_t info[8]);
  * a producer warp bulk-copies each tile's source rows and flags into shared-memory stages,
  * consumer warps update node pairs from there in packed FP32 -- with two CTAs of 8 consumer warps
  * (8) or one CTA of 12 (9) per SM; fused steps of lattices with nx % 16 == 0, nx <= 1024 (8) or
- * 1536 (9) and the pair kernels' plan conditions, else variant 5 runs. */
+ * 1536 (9) and the pair kernels' plan conditions.  Other lattices with nx >= 4, fewer than 2^32
+ * nodes and those plan conditions take the span pipeline at the same shape: tiles are spans of
+ * the linear node index, one bulk copy per direction, so rows of any length stream from shared
+ * memory.  Otherwise variant 5 runs. */
 #define HLBM_NUM_VARIANTS 10
 int hlbm_tune(hlbm_ctx* ctx, int32_t variant);
 int hlbm_autotune(hlbm_ctx* ctx, int32_t reps, int32_t* chosen, double* ms_per_variant);
