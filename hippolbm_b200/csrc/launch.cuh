@@ -40,6 +40,7 @@ cudaError_t launch_faces(const S* fi, S* fo, const int8_t* flags, const StepPlan
       const int64_t a = f < 2 ? int64_t(p.ny) * p.nz : (f < 4 ? int64_t(p.nx) * p.nz : int64_t(p.nx) * p.ny);
       area = a > area ? a : area;
     }
+  if ((faces & 3) == 3 && 2 * int64_t(p.ny) * p.nz > area) area = 2 * int64_t(p.ny) * p.nz;  // x faces interleaved
   const dim3 fgrid(unsigned((area + 255) / 256), 6, 1);
   if (MODE == MODE_FUSED && p.collision == 0)
     k_faces<S, R, STRICT, MODE, WALLS, 0><<<fgrid, 256, 0, s>>>(fi, fo, flags, p, faces);

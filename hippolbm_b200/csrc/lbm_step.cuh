@@ -1167,6 +1167,22 @@ __global__ void __launch_bounds__(256) k_faces(const S* __restrict__ fin, S* __r
                                                const int8_t* __restrict__ flags, const StepPlan p, int faces) {
   const int F = blockIdx.y;
   if (!(faces >> F & 1)) return;
+  if ((faces & 3) == 3 && F < 2) {
+    // both x faces in one interleaved sweep: thread i takes x = nx - 1 of row (i + 1) / 2 for even i
+    // and x = 0 of that row for odd i (row 0's x = 0 last), so neighbouring threads step nodes
+    // that are neighbours in memory (the end of one row, the start of the next) and share the
+    // sectors of their loads and stores; the two faces' nodes alone lie nx elements apart
+    if (F == 1) return;
+    const int64_t rows = int64_t(p.ny) * p.nz;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= 2 * rows) return;
+    int64_t r = (i + 1) >> 1;
+    const int x = ((i + 1) & 1) ? p.nx - 1 : 0;
+    if (r == rows) r = 0;
+    const int z = int(r / p.ny), y = int(r - int64_t(z) * p.ny);
+    node_step<S, R, STRICT, MODE, WALLS, COLL>(fin, fout, flags, p, x, y, z);
+    return;
+  }
   const int axis = F / 2;
   const int na = axis == 0 ? p.ny : p.nx;  // the face's two axes, in x, y, z order
   const int nb = axis == 2 ? p.ny : p.nz;
